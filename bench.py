@@ -1,0 +1,366 @@
+"""Benchmark: batched, checkpointed FWI gradient on one B200 per rank.
+
+Workload (one "step" = one full gradient of the survey): 64 surface shots on
+the 1000 x 300 three-layer model (h = 10 m, Ricker 8 Hz, dt = 0.8 ms,
+nt = 4000, order 4): forward modelling with checkpoints, L2 residual and
+misfit, checkpointed adjoint with Kahan-summed gradient.  Synthetic data
+(seeded model generator, observed gathers modelled on the true model).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
+
+Under torchrun each rank runs its own 64 shots of a 64*N-shot survey
+(weak scaling) and the shot-summed gradient and misfit are all-reduced with
+NCCL.  Rank 0 prints one JSON line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+NX, NZ, NT, NSHOTS = 1000, 300, 4000, 64
+ALG_BYTES = {0: 16, 1: 20, 2: 28}      # per cell-update: forward, recompute, adjoint
+MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjoint step (+gradient)"}
+
+
+def _peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id = gpu_id
+        self.proc = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except Exception:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------
+# reference CPU implementation (the reference's own propagator, compiled from
+# its sources into oracle/_ref) -- the CPU baseline and the reference arm
+# ----------------------------------------------------------------------------
+
+def cpu_reference_shot_gradient(survey, k):
+    """One shot-gradient with the reference's compiled CPU propagator."""
+    import oracle as O
+
+    obs = O.shot_gather(survey.vel, survey.w, survey.h, survey.dt, 4, survey.sx[k], survey.sy[k],
+                        survey.ry[k], backend="ref")
+    t0 = time.perf_counter()
+    O.shot_gradient(survey.vel_start, survey.w, survey.h, survey.dt, 4, survey.sx[k], survey.sy[k],
+                    survey.ry[k], lambda f: (f - obs).astype(np.float32), backend="ref")
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(survey, nsample=1):
+    import oracle as O
+
+    kind = "reference" if O.have_ref() else "port"
+    if kind == "port":
+        return None
+    cores = os.cpu_count() or 1
+    secs = [cpu_reference_shot_gradient(survey, 31 + i) for i in range(nsample)]
+    return {"value": nsample / sum(secs), "unit": "shot-gradients/s", "cores": cores, "kind": kind,
+            "sample": f"{nsample} shot-gradient(s) of the 1000x300 nt=4000 survey "
+                      f"(forward + adjoint, reference CPU propagator, OMP_NUM_THREADS={cores})"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from torchwi_b200 import synthetic
+    import oracle as O
+
+    survey = synthetic.config2(nshots=NSHOTS, nt=NT)
+    cores = os.cpu_count() or 1
+    if not O.have_ref():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference CPU propagator (oracle/_ref) not built"}))
+        return
+    for i in range(args.warmup):
+        cpu_reference_shot_gradient(survey, i % NSHOTS)
+    secs = [cpu_reference_shot_gradient(survey, i % NSHOTS) for i in range(args.steps)]
+    value = len(secs) / sum(secs)
+    line = {
+        "impl": "reference", "metric": "shot-gradients/s", "value": value, "unit": "shot-gradients/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config2 FWI gradient, 1000x300 cells, nt=4000, order 4; "
+                               "one shot per step (bounded sample of the 64-shot survey)",
+                   "parallelism": f"cpu openmp x{cores}"},
+        "cpu_baseline": {"value": value, "unit": "shot-gradients/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": "one shot-gradient per step, reference CPU propagator"},
+        "e2e": {"value": value, "unit": "shot-gradients/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------
+# B200 arm
+# ----------------------------------------------------------------------------
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from torchwi_b200 import PlanOptions, ShotPlan, synthetic
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    survey = synthetic.config2(nshots=NSHOTS * world, nt=NT)
+    mine = slice(rank * NSHOTS, (rank + 1) * NSHOTS)
+    sx, sy, ry = survey.sx[mine], survey.sy[mine], survey.ry[mine]
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
+                       shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True)
+    plan = ShotPlan(NX, NZ, survey.h, survey.dt, NT, 4, nshots=NSHOTS, options=opts, device=dev)
+    plan.set_wavelet(torch.from_numpy(survey.w))
+    plan.set_shots(sx, sy, ry)
+
+    # observed data: modelled on the true model (outside the timed region)
+    plan.set_model(torch.from_numpy(survey.vel).to(dev))
+    obs = plan.forward(save_checkpoints=False).clone()
+    vel0 = torch.from_numpy(survey.vel_start).to(dev)
+
+    def fwi_step(vel, obs_d):
+        plan.set_model(vel)
+        frd = plan.forward(save_checkpoints=True)
+        frd.sub_(obs_d)                       # residual, in the resid region
+        loss = 0.5 * frd.square().sum()
+        g = plan.gradient(None)
+        if world > 1:
+            dist.all_reduce(g)
+            dist.all_reduce(loss)
+        return loss, g
+
+    for _ in range(args.warmup):
+        fwi_step(vel0, obs)
+    plan.check()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+
+    def timed(fn, steps):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    with ClockSampler(uuid) as clk:
+        ms = timed(lambda: fwi_step(vel0, obs), args.steps)
+    plan.check()
+    clocks = clk.summary()
+    ms_step = ms / args.steps
+    total_shots = NSHOTS * world
+    value = total_shots / (ms_step / 1e3)
+    gcell = 2.0 * total_shots * NX * NZ * NT / (ms_step / 1e3) / 1e9
+
+    # end to end: host inputs (pinned), H2D copies and D2H of the result in the region
+    vel_h = torch.from_numpy(survey.vel_start).pin_memory()
+    obs_h = obs.cpu().pin_memory()
+    g_h = torch.empty((NX, NZ), dtype=torch.float32).pin_memory()
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    vel_buf = torch.empty_like(vel0)
+    obs_buf = torch.empty_like(obs)
+
+    def e2e_step():
+        vel_buf.copy_(vel_h, non_blocking=True)
+        obs_buf.copy_(obs_h, non_blocking=True)
+        loss, g = fwi_step(vel_buf, obs_buf)
+        g_h.copy_(g, non_blocking=True)
+        loss_h.copy_(loss, non_blocking=True)
+
+    e2e_step()
+    ms_e2e = timed(e2e_step, max(1, args.steps // 2)) / max(1, args.steps // 2)
+    h2d = vel_h.numel() * 4 + obs_h.numel() * 4
+    d2h = g_h.numel() * 4 + 4
+
+    # per-kernel device time at steady state -> roofline of the dominant kernel
+    ms_launch = {m: plan.profile(m, repeats=args.profile_reps) for m in (0, 1, 2)}
+    dom = max(ms_launch, key=lambda m: ms_launch[m])
+    cells = NSHOTS * NX * NZ
+    achieved = ALG_BYTES[dom] * cells / (ms_launch[dom] / 1e3) / 1e9
+    peak, peak_kind = _peak_hbm()
+    traffic = None
+    tpath = os.path.join(REPO, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                traffic = json.load(f).get(str(dom))
+        except Exception:
+            traffic = None
+
+    # the plain form: one shot per launch sequence, no graphs, no batching
+    plain = None
+    if args.plain_shots > 0 and rank == 0:
+        popts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
+                            shots_per_cta=1, use_graphs=False)
+        p1 = ShotPlan(NX, NZ, survey.h, survey.dt, NT, 4, nshots=1, options=popts, device=dev)
+        p1.set_wavelet(torch.from_numpy(survey.w))
+
+        def plain_run(nsh):
+            acc = torch.zeros((NX, NZ), device=dev)
+            for k in range(nsh):
+                p1.set_shots(sx[k:k + 1], sy[k:k + 1], ry[k:k + 1])
+                p1.set_model(vel0)
+                f = p1.forward(True)
+                f.sub_(obs[k:k + 1])
+                acc += p1.gradient(None)
+            return acc
+
+        plain_run(1)
+        ms_plain = timed(lambda: plain_run(args.plain_shots), 1) if world == 1 else None
+        if ms_plain:
+            plain = {"value": args.plain_shots / (ms_plain / 1e3), "unit": "shot-gradients/s",
+                     "shots_timed": args.plain_shots}
+        del p1
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(survey, nsample=1)
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        launches = args.steps * (3 * NT + 2)   # pad + forward nt + recompute nt + adjoint nt + reduce
+        line = {
+            "metric": "shot-gradients/s", "value": value, "unit": "shot-gradients/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded 3-layer model, observed gathers modelled on the true model)",
+            "config": {"workload": "config2: batched checkpointed FWI gradient, 64 shots/GPU, "
+                                   "1000x300 cells, nt=4000, order 4, Keys ABC, Kahan gradient",
+                       "global_batch": total_shots, "parallelism": f"shots sharded over {world} GPU(s)",
+                       "arith": "fast-fp32" if args.fast else "reference-exact",
+                       "ckpt_interval": plan.layout.ckpt_interval,
+                       "shots_per_cta": plan.layout.shots_per_cta,
+                       "rows_per_warp": plan.layout.rows_per_warp,
+                       "l2": "inputs larger than L2 (workspace %.1f GB)" % (plan.workspace.numel() / 1e9)},
+            "gcell_per_s": gcell,
+            "clocks": clocks,
+            "e2e": {"value": total_shots / (ms_e2e / 1e3), "unit": "shot-gradients/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": MODE_NAMES[dom], "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
+                         "ms_per_launch": {MODE_NAMES[m]: v for m, v in ms_launch.items()}},
+            "plain_form": plain,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    global NSHOTS, NT
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--fast", action="store_true", help="fast FP32 arithmetic instead of exact")
+    ap.add_argument("--ckpt", type=int, default=0)
+    ap.add_argument("--spc", type=int, default=0)
+    ap.add_argument("--rz", type=int, default=0)
+    ap.add_argument("--plain-shots", type=int, default=4)
+    ap.add_argument("--profile-reps", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shots", type=int, default=NSHOTS, help="shots per GPU")
+    ap.add_argument("--nt", type=int, default=NT, help="time steps")
+    args = ap.parse_args()
+    NSHOTS, NT = args.shots, args.nt
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

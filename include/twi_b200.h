@@ -1,0 +1,154 @@
+/* twi_b200.h -- C ABI of the B200 time-domain 2D acoustic propagator.
+ *
+ * Plain C types only: device pointers are `void*`/`float*` into memory the
+ * caller owns (PyTorch tensors in the Python layer), streams are
+ * `cudaStream_t` passed as `void*` (NULL = legacy default stream).  Every
+ * function returns an int status; on failure twi_last_error() returns a
+ * message for the calling thread.
+ *
+ * Two levels:
+ *   1. Reference-shaped entry points (twi_fdm_*) with the argument lists of
+ *      TorchWI's native propagator functions, for code that binds those
+ *      directly.
+ *   2. The plan API: batched shots, checkpointed adjoint, Kahan-summed
+ *      gradient, CUDA-graph time loops.  This is what torchwi_b200.Time2d
+ *      uses.
+ */
+#ifndef TWI_B200_H
+#define TWI_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    TWI_OK = 0,
+    TWI_ERR_INVALID = 1, /* bad argument (order, sizes, shot/receiver position, ...) */
+    TWI_ERR_CUDA = 2,    /* a CUDA runtime call failed */
+    TWI_ERR_STATE = 3,   /* call out of sequence (e.g. gradient before forward) */
+    TWI_ERR_DEVICE = 4,  /* a kernel raised the device error word (bounded wait ran out) */
+    TWI_ERR_NOMEM = 5    /* workspace too small */
+};
+
+/* Library version (major*10000 + minor*100 + patch). */
+int twi_version(void);
+
+/* Message describing the last failure on this thread ("" if none). */
+const char* twi_last_error(void);
+
+/* ------------------------------------------------------------------------
+ * 1. Reference-shaped entry points
+ *
+ * Layout as in the reference: vel, u1, u2, u3 and grad are [dimy][dimx]
+ * (x fastest) with dimx = nx + order, dimy = ny + order; frd and resid are
+ * [nt][nx]; virt is [nt][dimy][dimx].  All array pointers are device
+ * pointers except `w`, which may be host or device memory (the reference
+ * keeps it on the host).  Semantics are those of the reference's CPU
+ * propagator (unpadded grid, Keys on left/right/bottom, free top), computed
+ * on the GPU with bit-identical FP32 results.  u1/u2/u3 are accepted for
+ * signature compatibility and left untouched; scratch is taken with
+ * cudaMallocAsync on `stream` and released before return.
+ * ------------------------------------------------------------------------ */
+
+/* Replaces c_fdm_forward / cuda_fdm_forward
+ * (torchwi/propagator/td2d/propagator_cpu.h:2-18,
+ *  torchwi/propagator/td2d/propagator_cuda.h:2-18; bound from Python in
+ *  wrapper_cuda.cpp:45-79). */
+int twi_fdm_forward(float* frd, float* virt, float* u1, float* u2, float* u3,
+                    const float* vel, const float* w, int order, int dimx, int dimy,
+                    int nt, float h, float dt, float sx, float sy, float ry,
+                    void* stream);
+
+/* Replaces c_fdm_backward / cuda_fdm_backward
+ * (propagator_cpu.h:20-34, propagator_cuda.h:21-35; wrapper_cuda.cpp:81-113).
+ * `grad` ([dimy][dimx]) is overwritten, not accumulated. */
+int twi_fdm_backward(float* grad, const float* virt, float* u1, float* u2, float* u3,
+                     const float* vel, const float* resid, int order, int dimx,
+                     int dimy, int nt, float h, float dt, float ry, void* stream);
+
+/* Replaces c_fdm_forward_only / cuda_fdm_forward_only
+ * (propagator_cpu.h:37-53, propagator_cuda.h:38-53;
+ *  wrapper_forward_cuda.cpp:30-61). */
+int twi_fdm_forward_only(float* frd, float* u1, float* u2, float* u3, const float* vel,
+                         const float* w, int order, int dimx, int dimy, int nt, float h,
+                         float dt, float sx, float sy, float ry, void* stream);
+
+/* ------------------------------------------------------------------------
+ * 2. Plan API
+ *
+ * Replaces the per-shot Time2d work buffers and the Python-side loop over
+ * shots (torchwi/operator/TimeOperator.py:18-82, TimeFunction.py:108-148,
+ * examples/time/inv_torch.py:128-137): one plan holds one model, `nshots`
+ * shots and a workspace the caller allocates.
+ * ------------------------------------------------------------------------ */
+
+typedef struct twi_problem {
+    int order;            /* 2, 4 or 8 (spatial accuracy) */
+    int nx, nz;           /* model cells (unpadded) */
+    int nt;               /* time steps */
+    float h, dt;          /* grid spacing [m], time step [s] */
+    int nshots;           /* shots advanced together */
+    int ckpt_interval;    /* steps between wavefield checkpoints; 0 = choose */
+    int exact;            /* 1: reference arithmetic (bit-identical to TorchWI's CPU
+                             propagator); 0: fast FP32 with FMA */
+    int accumulate;       /* 0: Kahan-compensated FP32 over steps and shots;
+                             1: plain FP32 per shot, summed in shot order (the
+                             reference's order: bit-identical gradients) */
+    int shots_per_cta;    /* shots sharing one velocity tile in a CTA; 0 = choose */
+    int rows_per_warp;    /* 4 or 8; 0 = choose */
+    int use_graphs;       /* 1: capture the time loops into CUDA graphs */
+    int wavelet_per_shot; /* 1: wavelet region is [nshots][nt]; 0: one [nt] */
+} twi_problem;
+
+/* Byte offsets of the caller-visible regions inside the workspace. */
+typedef struct twi_layout {
+    size_t workspace_bytes; /* total size to allocate (256-byte aligned base) */
+    size_t vel;             /* in : model (nx, nz), z fastest, float */
+    size_t wavelet;         /* in : [nshots or 1][nt] float */
+    size_t gathers;         /* out: [nshots][nt][nx] float (twi_forward) */
+    size_t resid;           /* in : [nshots][nt][nx] float adjoint source (twi_gradient) */
+    size_t grad;            /* out: (nx, nz) float, z fastest (twi_gradient) */
+    int dimx, dimz, pitch;  /* padded grid and its row pitch (floats) */
+    int ckpt_interval, nsegments, shots_per_cta, rows_per_warp;
+} twi_layout;
+
+typedef struct twi_plan twi_plan;
+
+/* Validate `prob` and size the workspace; no device memory is touched. */
+int twi_plan_create(const twi_problem* prob, twi_plan** plan);
+int twi_plan_layout(const twi_plan* plan, twi_layout* out);
+/* Attach a device workspace of at least layout.workspace_bytes bytes on the
+ * current device; drops captured graphs. */
+int twi_plan_bind(twi_plan* plan, void* workspace, size_t bytes);
+/* Shot and receiver positions in metres (host arrays of nshots floats);
+ * cells are (int)(coord/h) in FP32 as in propagator_cpu.cpp:44-48.  Shots
+ * must lie inside the model, receiver rows inside the grid. */
+int twi_plan_set_shots(twi_plan* plan, const float* sx, const float* sy, const float* ry,
+                       void* stream);
+/* Pad the model from the `vel` region into the internal grid. */
+int twi_plan_set_model(twi_plan* plan, void* stream);
+/* Forward pass for all shots: gathers -> `gathers`.  With save_checkpoints
+ * the wavefield pairs needed by twi_gradient are kept. */
+int twi_forward(twi_plan* plan, int save_checkpoints, void* stream);
+/* Adjoint pass for all shots from the `resid` region: recomputes the
+ * forward field segment by segment from the checkpoints and writes the
+ * shot-summed velocity gradient to `grad`. */
+int twi_gradient(twi_plan* plan, void* stream);
+/* Synchronise `stream` and report a raised device error word. */
+int twi_plan_check(twi_plan* plan, void* stream);
+/* Measurement hook (no counterpart in the reference): launch `repeats`
+ * steady-state time steps of one kernel mode (0 forward, 1 recompute with
+ * virtual-source output, 2 adjoint with gradient accumulation) for all shots
+ * and return the mean device time per launch in *ms_per_launch (CUDA events
+ * on `stream`).  Overwrites rotating wavefield slots and the gradient
+ * accumulators, never the checkpoints; call after twi_forward. */
+int twi_plan_profile(twi_plan* plan, int mode, int repeats, float* ms_per_launch, void* stream);
+int twi_plan_destroy(twi_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TWI_B200_H */

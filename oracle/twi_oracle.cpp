@@ -184,7 +184,7 @@ struct Grid {
 };
 
 // Cell index arithmetic of the reference: float division then truncation
-// (propagator_cpu.cpp:30-34).
+// (propagator_cpu.cpp:44-48).
 template <typename T>
 int cell_of(T coord, T h) { return static_cast<int>(coord / h); }
 

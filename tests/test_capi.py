@@ -1,0 +1,96 @@
+"""The C-ABI library loads, exports every symbol declared in include/*.h and
+validates problems on the host -- no GPU needed (no compute calls)."""
+import ctypes
+import glob
+import os
+import re
+
+import pytest
+
+from torchwi_b200 import _capi
+from torchwi_b200.build import LIB
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    names = set()
+    for h in glob.glob(os.path.join(REPO, "include", "*.h")):
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names.update(re.findall(r"^\s*(?:int|const char\*|void)\s+\**\s*(twi_\w+)\s*\(", src, re.M))
+    return sorted(names)
+
+
+def test_library_built_in_tree():
+    assert os.path.exists(LIB), "run python -m torchwi_b200.build"
+
+
+def test_exports_every_declared_symbol():
+    lib = ctypes.CDLL(LIB)
+    names = _declared_symbols()
+    assert len(names) >= 14
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_bindings_cover_header():
+    assert set(_declared_symbols()) <= set(_capi.SIGNATURES)
+
+
+def _problem(**kw):
+    base = dict(order=4, nx=100, nz=50, nt=200, h=10.0, dt=1e-3, nshots=4, ckpt_interval=0,
+                exact=1, accumulate=0, shots_per_cta=0, rows_per_warp=0, use_graphs=1,
+                wavelet_per_shot=0)
+    base.update(kw)
+    return _capi.Problem(**base)
+
+
+def _create(**kw):
+    L = _capi.lib()
+    h = ctypes.c_void_p()
+    st = L.twi_plan_create(ctypes.byref(_problem(**kw)), ctypes.byref(h))
+    return st, h
+
+
+def test_plan_layout_on_host():
+    L = _capi.lib()
+    st, h = _create(nt=4000, nshots=64, nx=1000, nz=300, ckpt_interval=50)
+    assert st == _capi.TWI_OK
+    lay = _capi.Layout()
+    assert L.twi_plan_layout(h, ctypes.byref(lay)) == 0
+    assert (lay.dimx, lay.dimz, lay.pitch) == (1004, 304, 1024)
+    assert lay.ckpt_interval == 50 and lay.nsegments == 80
+    # fields: (1 + 64*(6 + 2*79)) slots + 64*50 virtual-source slots, 1024*304 floats each
+    slot = 1024 * 304 * 4
+    assert lay.workspace_bytes >= (1 + 64 * 164 + 64 * 50) * slot
+    assert lay.workspace_bytes < (1 + 64 * 164 + 64 * 50 + 40) * slot + 2 * 64 * 4000 * 1000 * 4
+    assert lay.workspace_bytes % 256 == 0
+    assert L.twi_plan_destroy(h) == 0
+
+
+@pytest.mark.parametrize("bad", [dict(order=6), dict(nx=0), dict(nt=0), dict(nshots=0),
+                                 dict(h=0.0), dict(rows_per_warp=3), dict(ckpt_interval=1)])
+def test_plan_rejects_invalid_problem(bad):
+    st, h = _create(**bad)
+    assert st == _capi.TWI_ERR_INVALID
+    assert _capi.last_error()
+
+
+def test_calls_out_of_sequence_are_errors():
+    L = _capi.lib()
+    st, h = _create()
+    assert st == 0
+    assert L.twi_forward(h, 1, None) == _capi.TWI_ERR_STATE
+    assert L.twi_gradient(h, None) == _capi.TWI_ERR_STATE
+    assert "workspace" in _capi.last_error()
+    L.twi_plan_destroy(h)
+
+
+def test_default_checkpoint_interval_is_sqrt_2nt():
+    L = _capi.lib()
+    st, h = _create(nt=4000)
+    lay = _capi.Layout()
+    L.twi_plan_layout(h, ctypes.byref(lay))
+    assert lay.ckpt_interval == 89 and lay.nsegments == 45
+    L.twi_plan_destroy(h)

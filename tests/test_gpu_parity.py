@@ -1,0 +1,358 @@
+"""Parity of the CUDA path with the reference, through the C ABI.
+
+Bar: in reference-arithmetic mode (exact=True) gathers, virtual source and
+per-shot gradients are BIT-IDENTICAL to the reference CPU propagator (the
+oracle restatement, itself pinned bit-for-bit to the reference build and its
+golden vectors).  Kahan-accumulated gradients are within relative L2 1e-4 of
+the reference's plain-FP32 gradient; fast FP32
+mode is within 1e-5 (gathers) / 1e-4 (gradient).
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from golden_io import SMALL_CASES, bits_equal, load_json, load_small, rel_l2, sha
+from torchwi_b200 import PlanOptions, ShotPlan, Time2d, Time2dBatch, Time2dForward, synthetic
+from torchwi_b200.propagator import td2d_b200, td2d_forward_b200
+
+pytestmark = pytest.mark.gpu
+
+GATHER_TOL = 1e-5   # relative L2, gathers (fast mode)
+GRAD_TOL = 1e-4     # relative L2, gradients (Kahan / fast mode vs reference)
+
+
+def _oracle_shots(s, vel, shots=None, resid_fn=None, dtype=np.float32):
+    """Per-shot oracle gathers and (optionally) gradients on `vel`."""
+    shots = range(s.nshots) if shots is None else shots
+    out = []
+    for k in shots:
+        if resid_fn is None:
+            out.append(O.shot_gather(vel, s.w, s.h, s.dt, s.order, s.sx[k], s.sy[k], s.ry[k],
+                                     dtype=dtype))
+        else:
+            out.append(O.shot_gradient(vel, s.w, s.h, s.dt, s.order, s.sx[k], s.sy[k], s.ry[k],
+                                       lambda f, k=k: resid_fn(k, f), dtype=dtype))
+    return out
+
+
+def _plan(s, **kw):
+    opts = PlanOptions(**kw)
+    p = ShotPlan(s.nx, s.nz, s.h, s.dt, s.nt, s.order, nshots=s.nshots, options=opts)
+    p.set_wavelet(torch.from_numpy(s.w))
+    p.set_shots(s.sx, s.sy, s.ry)
+    return p
+
+
+# ----------------------------------------------------------------------------
+# drop-in native module (reference layout, reference-shaped C entry points)
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("order", [2, 4, 8])
+@pytest.mark.parametrize("shape", [(40, 24, 150), (37, 23, 130), (130, 41, 90)])
+def test_native_forward_backward_bitexact(order, shape):
+    nx, nz, nt = shape
+    s = synthetic.small_case(nx=nx, nz=nz, nt=nt, order=order, nshots=1, seed=nx + order)
+    dimx, dimy = nx + order, nz + order
+    vpad = O.pad_model(s.vel, order)
+    args = (order, dimx, dimy, nt, s.h, s.dt, s.sx[0], s.sy[0], s.ry[0])
+    f_or, v_or = O.twio_forward(vpad, s.w, *args)
+    dev = torch.device("cuda")
+    frd = torch.zeros(nt * nx, device=dev)
+    virt = torch.zeros(nt * dimx * dimy, device=dev)
+    u = [torch.zeros(dimx * dimy, device=dev) for _ in range(3)]
+    vp = torch.from_numpy(vpad).to(dev)
+    td2d_b200.forward(frd, virt, *u, vp, torch.from_numpy(s.w), *args)
+    assert bits_equal(frd.cpu().numpy().reshape(nt, nx), f_or)
+    assert bits_equal(virt.cpu().numpy().reshape(nt, -1), v_or)
+    resid = (0.3 * f_or + 0.01).astype(np.float32)
+    g_or = O.twio_backward(v_or, vpad, resid, order, dimx, dimy, nt, s.h, s.dt, s.ry[0])
+    g = td2d_b200.backward(virt, *u, vp, torch.from_numpy(resid).to(dev).reshape(-1), order,
+                           dimx, dimy, nt, s.h, s.dt, s.ry[0])
+    assert bits_equal(g.cpu().numpy(), g_or)
+    # forward-only module
+    frd2 = torch.zeros_like(frd)
+    td2d_forward_b200.forward(frd2, *u, vp, torch.from_numpy(s.w).cuda(), *args)
+    assert bits_equal(frd2.cpu().numpy().reshape(nt, nx), f_or)
+
+
+def test_native_rejects_bad_input():
+    dev = torch.device("cuda")
+    z = torch.zeros(64 * 44, device=dev)
+    w = torch.zeros(10)
+    with pytest.raises(RuntimeError):
+        td2d_b200.forward(torch.zeros(10 * 40, device=dev), torch.zeros(10 * 64 * 44, device=dev),
+                          z, z, z, z, w, 6, 44, 64, 10, 10.0, 1e-3, 10.0, 20.0, 20.0)
+    with pytest.raises(RuntimeError):   # shot outside the model
+        td2d_b200.forward(torch.zeros(10 * 40, device=dev), torch.zeros(10 * 64 * 44, device=dev),
+                          z, z, z, z, w, 4, 44, 64, 10, 10.0, 1e-3, 5000.0, 20.0, 20.0)
+    with pytest.raises(RuntimeError):   # not a CUDA tensor
+        td2d_b200.forward(torch.zeros(10 * 40), z, z, z, z, z, w, 4, 44, 64, 10, 10.0, 1e-3,
+                          10.0, 20.0, 20.0)
+
+
+# ----------------------------------------------------------------------------
+# plan API: batched shots, checkpointed adjoint
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("order", [2, 4, 8])
+def test_plan_gathers_bitexact(order):
+    s = synthetic.small_case(nx=150, nz=45, nt=160, order=order, nshots=5, seed=3)
+    p = _plan(s)
+    p.set_model(torch.from_numpy(s.vel))
+    g = p.forward(save_checkpoints=False).cpu().numpy()
+    ref = _oracle_shots(s, s.vel)
+    for k in range(s.nshots):
+        assert bits_equal(g[k], ref[k]), k
+
+
+@pytest.mark.parametrize("order", [2, 4, 8])
+@pytest.mark.parametrize("K", [2, 7, 0])
+def test_plan_gradient_plain_bitexact(order, K):
+    """accumulate='plain': per-shot FP32 sums added in shot order, exactly as
+    the reference inversion loop accumulates par.grad."""
+    s = synthetic.small_case(nx=70, nz=33, nt=120, order=order, nshots=3, seed=11)
+    obs = _oracle_shots(s, s.vel)
+    res = _oracle_shots(s, s.vel_start, resid_fn=lambda k, f: (f - obs[k]).astype(np.float32))
+    g_ref = res[0][1]
+    for k in range(1, s.nshots):
+        g_ref = (g_ref + res[k][1]).astype(np.float32)
+    p = _plan(s, accumulate="plain", ckpt_interval=K)
+    p.set_model(torch.from_numpy(s.vel_start))
+    frd = p.forward(save_checkpoints=True).clone()
+    for k in range(s.nshots):
+        assert bits_equal(frd[k].cpu().numpy(), res[k][0])
+    resid = frd - torch.from_numpy(np.stack(obs)).cuda()
+    g = p.gradient(resid).cpu().numpy()
+    p.check()
+    assert bits_equal(g, g_ref)
+
+
+@pytest.mark.parametrize("spc", [1, 2, 4])
+def test_plan_gradient_kahan(spc):
+    s = synthetic.small_case(nx=90, nz=40, nt=200, order=4, nshots=4, seed=5)
+    obs = _oracle_shots(s, s.vel)
+    res = _oracle_shots(s, s.vel_start, resid_fn=lambda k, f: (f - obs[k]).astype(np.float32))
+    g_ref = res[0][1]
+    for k in range(1, s.nshots):
+        g_ref = (g_ref + res[k][1]).astype(np.float32)
+    res64 = _oracle_shots(s, s.vel_start.astype(np.float64),
+                          resid_fn=lambda k, f: f - obs[k].astype(np.float64), dtype=np.float64)
+    g64 = sum(r[1] for r in res64)
+    p = _plan(s, accumulate="kahan", shots_per_cta=spc, ckpt_interval=9)
+    p.set_model(torch.from_numpy(s.vel_start))
+    frd = p.forward()
+    resid = frd - torch.from_numpy(np.stack(obs)).cuda()
+    g = p.gradient(resid).cpu().numpy()
+    p.check()
+    assert rel_l2(g, g_ref) <= GRAD_TOL
+    # compensated sums are at least as close to FP64 as the reference's plain sums
+    assert rel_l2(g, g64) <= rel_l2(g_ref, g64) * 1.5 + 1e-7
+
+
+def test_plan_fast_mode_within_tolerance():
+    s = synthetic.small_case(nx=100, nz=50, nt=300, order=4, nshots=2, seed=9)
+    obs = _oracle_shots(s, s.vel)
+    res = _oracle_shots(s, s.vel_start, resid_fn=lambda k, f: (f - obs[k]).astype(np.float32))
+    p = _plan(s, exact=False)
+    p.set_model(torch.from_numpy(s.vel_start))
+    frd = p.forward()
+    for k in range(s.nshots):
+        assert rel_l2(frd[k].cpu().numpy(), res[k][0]) <= GATHER_TOL
+    g = p.gradient(frd - torch.from_numpy(np.stack(obs)).cuda()).cpu().numpy()
+    assert rel_l2(g, res[0][1] + res[1][1]) <= GRAD_TOL
+
+
+def test_graphs_and_direct_launches_agree():
+    s = synthetic.small_case(nx=60, nz=30, nt=90, order=4, nshots=2, seed=1)
+    out = []
+    for graphs in (True, False):
+        p = _plan(s, use_graphs=graphs)
+        p.set_model(torch.from_numpy(s.vel_start))
+        frd = p.forward().clone()
+        g = p.gradient(0.5 * frd).clone()
+        out.append((frd.cpu().numpy(), g.cpu().numpy()))
+        # replay (graph path reuses the captured graphs)
+        frd2 = p.forward().clone()
+        assert bits_equal(frd2.cpu().numpy(), out[-1][0])
+    assert bits_equal(out[0][0], out[1][0]) and bits_equal(out[0][1], out[1][1])
+
+
+def test_rows_per_warp_variants_agree():
+    s = synthetic.small_case(nx=80, nz=70, nt=100, order=8, nshots=2, seed=2)
+    res = []
+    for rz in (4, 8):
+        p = _plan(s, rows_per_warp=rz, accumulate="plain")
+        p.set_model(torch.from_numpy(s.vel_start))
+        frd = p.forward().clone()
+        res.append((frd.cpu().numpy(), p.gradient(frd).cpu().numpy()))
+    assert bits_equal(res[0][0], res[1][0]) and bits_equal(res[0][1], res[1][1])
+
+
+def test_plan_rejects_bad_shot():
+    s = synthetic.small_case(nx=30, nz=20, nt=20, order=4, nshots=1)
+    p = _plan(s)
+    from torchwi_b200 import TwiInvalid
+    with pytest.raises(TwiInvalid):
+        p.set_shots([1e6], [20.0], [20.0])
+    with pytest.raises(TwiInvalid):
+        p.set_shots([10.0], [20.0], [1e6])
+
+
+def test_gradient_before_forward_is_an_error():
+    s = synthetic.small_case(nx=30, nz=20, nt=20, order=4, nshots=1)
+    p = _plan(s)
+    p.set_model(torch.from_numpy(s.vel))
+    from torchwi_b200 import TwiError
+    with pytest.raises(TwiError):
+        p.gradient(torch.zeros(1, s.nt, s.nx))
+
+
+# ----------------------------------------------------------------------------
+# operator mirror against the golden vectors of the reference operator
+# ----------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("accumulate", ["plain", "kahan"])
+def test_time2d_against_reference_golden(name, accumulate):
+    g = load_small(name)
+    nx, nz = g["vel"].shape
+    w = torch.from_numpy(g["w"])
+    model = Time2d(nx, nz, g["h"], w, g["dt"], g["order"], "cuda",
+                   options=PlanOptions(accumulate=accumulate))
+    vel = torch.from_numpy(g["vel"]).cuda()
+    par = torch.nn.Parameter(torch.from_numpy(g["vel_start"]).cuda())
+    for k in range(len(g["sx"])):
+        sx, sy, ry = (torch.tensor(g[c][k]) for c in ("sx", "sy", "ry"))
+        with torch.no_grad():
+            obs = model(vel, sx, sy, ry)
+        assert bits_equal(obs.cpu().numpy(), g["obs"][k])
+        frd = model(par, sx, sy, ry)
+        assert bits_equal(frd.detach().cpu().numpy(), g["frd"][k])
+        loss = 0.5 * torch.sum((frd - torch.from_numpy(g["obs"][k]).cuda()) ** 2)
+        loss.backward()
+    grad = par.grad.cpu().numpy()
+    if accumulate == "plain":
+        assert bits_equal(grad, g["grad"])
+    else:
+        assert rel_l2(grad, g["grad"]) <= GRAD_TOL
+
+
+def test_time2d_backward_after_interleaved_forward():
+    """The reference returns a view of a reused buffer and cannot take two
+    forwards before a backward; this operator recomputes instead."""
+    g = load_small("small_o4")
+    nx, nz = g["vel"].shape
+    model = Time2d(nx, nz, g["h"], torch.from_numpy(g["w"]), g["dt"], 4, "cuda",
+                   options=PlanOptions(accumulate="plain"))
+    par = torch.nn.Parameter(torch.from_numpy(g["vel_start"]).cuda())
+    losses = []
+    for k in range(2):
+        sx, sy, ry = (torch.tensor(g[c][k]) for c in ("sx", "sy", "ry"))
+        frd = model(par, sx, sy, ry)
+        losses.append(0.5 * torch.sum((frd - torch.from_numpy(g["obs"][k]).cuda()) ** 2))
+    (losses[0] + losses[1]).backward()
+    assert rel_l2(par.grad.cpu().numpy(), g["grad"]) <= 1e-6
+
+
+def test_time2d_forward_config1_hashes():
+    rec = load_json("config1.json")
+    s = synthetic.config1()
+    model = Time2dForward(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, s.order, "cuda")
+    vel = torch.from_numpy(s.vel).cuda()
+    for k, shot in enumerate(rec["shots"]):
+        with torch.no_grad():
+            gth = model(vel, torch.tensor(s.sx[k]), torch.tensor(s.sy[k]), torch.tensor(s.ry[k]))
+        assert sha(gth.cpu().numpy()) == shot["sha256"], k
+
+
+def test_batch_operator_matches_plan_and_time2d():
+    s = synthetic.small_case(nx=64, nz=32, nt=150, order=4, nshots=3, seed=4)
+    obs = torch.from_numpy(np.stack(_oracle_shots(s, s.vel))).cuda()
+    opts = PlanOptions(accumulate="plain")
+    m = Time2dBatch(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, 4, s.nshots, "cuda", options=opts)
+    par = torch.nn.Parameter(torch.from_numpy(s.vel_start).cuda())
+    frd = m(par, torch.from_numpy(s.sx), torch.from_numpy(s.sy), torch.from_numpy(s.ry))
+    (0.5 * ((frd - obs) ** 2).sum()).backward()
+    gb = par.grad.cpu().numpy()
+    t = Time2d(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, 4, "cuda", options=opts)
+    par2 = torch.nn.Parameter(torch.from_numpy(s.vel_start).cuda())
+    for k in range(s.nshots):
+        f = t(par2, torch.tensor(s.sx[k]), torch.tensor(s.sy[k]), torch.tensor(s.ry[k]))
+        (0.5 * ((f - obs[k]) ** 2).sum()).backward()
+    assert bits_equal(gb, par2.grad.cpu().numpy())
+
+
+# ----------------------------------------------------------------------------
+# full size (1000 x 300, nt = 4000): the reference's own gradient, by hash
+# ----------------------------------------------------------------------------
+
+@pytest.mark.slow
+def test_config2_shot_full_size():
+    rec = load_json("config2_shot.json")
+    s = synthetic.config2(nshots=64, nt=4000)
+    k = rec["shot"]
+    sx, sy, ry = (torch.tensor(a[k]) for a in (s.sx, s.sy, s.ry))
+    model = Time2d(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, 4, "cuda",
+                   options=PlanOptions(accumulate="plain"))
+    with torch.no_grad():
+        obs = model(torch.from_numpy(s.vel).cuda(), sx, sy, ry)
+    assert sha(obs.cpu().numpy()) == rec["obs_sha256"]
+    par = torch.nn.Parameter(torch.from_numpy(s.vel_start).cuda())
+    frd = model(par, sx, sy, ry)
+    assert sha(frd.detach().cpu().numpy()) == rec["frd_sha256"]
+    (0.5 * torch.sum((frd - obs) ** 2)).backward()
+    assert sha(par.grad.cpu().numpy()) == rec["grad_sha256"]
+    # Kahan mode: within the gradient tolerance of the reference's gradient
+    model_k = Time2d(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, 4, "cuda")
+    par_k = torch.nn.Parameter(torch.from_numpy(s.vel_start).cuda())
+    frd_k = model_k(par_k, sx, sy, ry)
+    (0.5 * torch.sum((frd_k - obs) ** 2)).backward()
+    err = rel_l2(par_k.grad.cpu().numpy(), par.grad.cpu().numpy())
+    print(f"config2 shot: Kahan vs reference gradient rel L2 = {err:.3e}")
+    assert err <= GRAD_TOL
+
+
+def test_finite_difference_of_misfit():
+    """<g, dv> against central differences of 0.5||d(v) - d_obs||^2 along
+    random smooth perturbations.  The reference's adjoint is a time-reversed
+    continuous adjoint, not the exact discrete one, and it discards the
+    gradient that lands in the edge-replicated pad cells
+    (TimeFunction.py:143-145).  The perturbations therefore vanish near the
+    left/right/bottom edges, and dt is fine (0.5 ms) so that the reference
+    scheme itself agrees with FD to <0.5% (measured with the FP64 oracle on
+    this case: 0.9972, 0.9955, 0.9992); tolerance 2e-2."""
+    from scipy.ndimage import gaussian_filter
+
+    s = synthetic.small_case(nx=120, nz=60, nt=800, order=4, nshots=2, seed=21, freq=8.0,
+                             dt=0.5e-3)
+    dev = torch.device("cuda")
+    m = Time2dBatch(s.nx, s.nz, s.h, torch.from_numpy(s.w), s.dt, 4, s.nshots, dev)
+    args = [torch.from_numpy(a) for a in (s.sx, s.sy, s.ry)]
+    with torch.no_grad():
+        obs = m(torch.from_numpy(s.vel).to(dev), *args).clone()
+    par = torch.nn.Parameter(torch.from_numpy(s.vel_start).to(dev))
+    frd = m(par, *args)
+    (0.5 * ((frd - obs) ** 2).sum()).backward()
+    g = par.grad.double()
+
+    def misfit(v):
+        with torch.no_grad():
+            f = m(v.float(), *args)
+            return 0.5 * ((f.double() - obs.double()) ** 2).sum().item()
+
+    rng = np.random.default_rng(0)
+    taper = 12
+    wx, wz = np.ones(s.nx), np.ones(s.nz)
+    wx[:taper] = 0
+    wx[-taper:] = 0
+    wz[-taper:] = 0
+    wz[:4] = 0
+    wx, wz = gaussian_filter(wx, 3), gaussian_filter(wz, 3)
+    for trial in range(3):
+        dv = gaussian_filter(rng.standard_normal((s.nx, s.nz)), 5.0) * wx[:, None] * wz[None, :]
+        dv = torch.from_numpy(dv / np.abs(dv).max() * 20.0).to(dev)   # up to 20 m/s
+        eps = 0.5
+        fd = (misfit(par.double() + eps * dv) - misfit(par.double() - eps * dv)) / (2 * eps)
+        an = float((g * dv).sum())
+        assert abs(fd / an - 1.0) < 2e-2, (trial, fd, an)

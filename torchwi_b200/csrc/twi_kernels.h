@@ -1,0 +1,101 @@
+// twi_kernels.h -- launch-level interface between the host planner
+// (twi_plan.cu) and the time-step kernels (twi_step.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+namespace twi {
+
+// What one launch of the step kernel does for each shot it owns.
+enum StepMode : int {
+    kModeForward = 0,     // u^{n+1}; point source; optional receiver gather
+    kModeRecompute = 1,   // u^{n+1}; point source; virtual source written out
+    kModeAdjoint = 2,     // lambda step; adjoint source on the receiver row;
+                          // gradient term accumulated
+};
+
+// Gradient accumulator layout used by kModeAdjoint.
+enum AccMode : int {
+    kAccNone = 0,
+    kAccPlainPerShot = 1,   // acc[shot] += term  (reference summation order)
+    kAccKahanPerGroup = 2,  // Kahan pair (acc, comp)[group] over steps and shots
+};
+
+// Geometry: the padded grid has dimz rows of dimx cells stored with a row
+// pitch of `pitch` floats (a multiple of 128); ne = order/2 pad cells on
+// every side; nx, nz are the model dimensions.  Wavefields live in "slots"
+// of pitch*dimz floats; slot(shot) = base + shot*stride.
+struct StepArgs {
+    int dimx, dimz, pitch, nx, nz;
+    long long slot_elems;
+    float* fields;
+    int prev_base, prev_stride;
+    int cur_base, cur_stride;
+    int next_base, next_stride;
+    int nshots;   // shots in this launch (grid.z * spc covers them)
+    int spc;      // shots per CTA
+    int it;       // time index of this step
+    float dtoh2, dt2, h2, hdt, cons;
+    // point source (modes 0, 1): src_rc[2*s] = padded row, [2*s+1] = column
+    const int* src_rc;
+    const float* wav;
+    long long wav_stride;       // wav[s*wav_stride + it]
+    // receivers: padded row per shot
+    const int* rec_row;
+    float* frd;                 // gathers (mode 0, may be null)
+    long long frd_stride;       // frd[s*frd_stride + it*nx + ix]
+    // adjoint source (mode 2)
+    const float* resid;
+    long long resid_stride;     // resid[s*resid_stride + it*nx + ix]
+    // virtual source out (mode 1) / in (mode 2): element (slot, r, c) at
+    // virt[(slot)*virt_slot_elems + r*virt_pitch + c]
+    float* virt_out;
+    const float* virt_in;
+    long long virt_slot_elems;
+    int virt_pitch;
+    int virt_base, virt_stride;
+    int virt_vec4;              // 1 when float4 access is aligned
+    // gradient accumulators (mode 2), same pitch/slot size as the fields
+    float* acc;
+    float* acc_comp;
+    int acc_mode;
+    int acc_base;               // slot of group 0 / shot 0
+    int* err;                   // device error word (bit 0: TMA wait timeout)
+};
+
+struct LaunchShape {
+    int rows_per_warp;   // 4 or 8
+    int warps;           // warps per CTA, stacked along z
+};
+
+// Launches one time step.  tm_u2 / tm_u1 / tm_vel are tensor maps over the
+// field slots (boxes with halo) and the padded velocity.
+cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
+                        const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
+                        const CUtensorMap& tm_vel, const StepArgs& a, cudaStream_t stream);
+
+// Set kernel attributes for all modes of (order, exact, shape) on the current
+// device.  Must run before a stream capture that launches them.
+cudaError_t prepare_step(int order, bool exact, LaunchShape shape);
+
+// Tile geometry shared by host and device.
+constexpr int kTileX = 128;                    // columns per CTA (32 lanes x float4)
+constexpr int kHaloX = 4;                      // x halo, keeps TMA x origins 16-byte aligned
+constexpr int kBoxX = kTileX + 2 * kHaloX;     // 136 columns per staged row
+__host__ __device__ constexpr int zhalo(int order) { return order / 2 > 2 ? order / 2 : 2; }
+
+// (nx, nz) z-fastest user model -> padded [dimz][pitch] x-fastest,
+// edge-replicated by ne cells (TimeOperator.py:55-58); columns >= dimx are 0.
+cudaError_t launch_pad_model(const float* vel_user, float* vpad, int nx, int nz, int ne,
+                             int dimx, int dimz, int pitch, cudaStream_t stream);
+
+// Combine gradient accumulators and write the (nx, nz) z-fastest result:
+// plain mode sums slots 0..nacc-1 in order; Kahan mode adds every slot's
+// (sum, -comp) pair with compensation.
+cudaError_t launch_reduce_grad(const float* acc, const float* acc_comp, int nacc,
+                               long long slot_elems, int pitch, int ne, int nx, int nz,
+                               int kahan, float* grad_user, cudaStream_t stream);
+
+}  // namespace twi

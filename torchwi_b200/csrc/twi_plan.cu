@@ -1,0 +1,737 @@
+// twi_plan.cu -- host side of the C ABI declared in include/twi_b200.h.
+//
+// A plan owns no device memory: the caller binds a workspace (a PyTorch
+// tensor in the Python layer) whose layout is computed here.  Wavefields
+// live in "slots" of pitch*dimz floats addressed through one 3-D TMA tensor
+// map; which slot holds u^k is decided by the schedule below, so the forward
+// pass writes each checkpointed field straight into its checkpoint slot
+// (no copies) and the recompute/adjoint passes read them back in place.
+//
+// Slot map of one shot (SPS slots per shot, global slot 0 is all zeros and
+// stands for u^{-1} = u^0 = lambda^{-1} = lambda^{-2} = 0):
+//   1 + s*SPS + {0,1,2}          forward/recompute rotation  u^k, k mod 3
+//   1 + s*SPS + {3,4,5}          adjoint rotation            lambda
+//   1 + s*SPS + 6 + 2(j-1) + p   checkpoint j >= 1: p=0 -> u^{jK-1}, p=1 -> u^{jK}
+// Gradient pass, segment j = nseg-1 .. 0 (K steps each, the last may be
+// shorter): recompute u^{jK+1..jK+L} from checkpoint j writing the virtual
+// source of each step into a K-slot buffer per shot, then run the L adjoint
+// steps backwards reading it.  One extra forward propagation in total.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "twi_b200.h"
+#include "twi_kernels.h"
+
+using namespace twi;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define TWI_CUDA(expr)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (expr);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(TWI_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TWI_TRY(expr)                 \
+    do {                              \
+        int s_ = (expr);              \
+        if (s_ != TWI_OK) return s_;  \
+    } while (0)
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// Tensor map over `nslots` slots of [dimz][pitch] floats (x extent dimx, so
+// reads past the last column return zeros); nslots == 0 gives a 2-D map.
+int make_map(CUtensorMap* tm, const void* base, int dimx, int dimz, long long nslots, int pitch,
+             int box_x, int box_z) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) return fail(TWI_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    const int rank = nslots > 0 ? 3 : 2;
+    cuuint64_t dims[3] = {(cuuint64_t)dimx, (cuuint64_t)dimz, (cuuint64_t)(nslots > 0 ? nslots : 1)};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * dimz * 4};
+    cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_z, 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<void*>(base), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(TWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return TWI_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Slot {
+    int base, stride;
+};
+
+// Cell lookup exactly as the reference: FP32 division, truncation toward 0
+// (propagator_cpu.cpp:44-48).
+int cell_of(float coord, float h) { return static_cast<int>(coord / h); }
+
+int check_order(int order) {
+    if (order != 2 && order != 4 && order != 8)
+        return fail(TWI_ERR_INVALID, "order must be 2, 4 or 8 (got " + std::to_string(order) + ")");
+    return TWI_OK;
+}
+
+// Shot/receiver cells in padded coordinates; the shot must be inside the
+// model and the receiver row inside the grid (the reference would index out
+// of bounds otherwise; its numba path raises for shots outside the model,
+// td2d_numba.py:45-49).
+int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, int dimz,
+               int* src_r, int* src_c, int* rec_r) {
+    const int isx = cell_of(sx, h), isy = cell_of(sy, h), iry = cell_of(ry, h);
+    if (!(sx >= 0.f) || !(sy >= 0.f) || isx >= nx || isy >= nz)
+        return fail(TWI_ERR_INVALID, "shot position outside the model: isx=" + std::to_string(isx) +
+                                         " isy=" + std::to_string(isy));
+    if (!(ry >= 0.f) || iry + ne >= dimz)
+        return fail(TWI_ERR_INVALID, "receiver row outside the grid: iry=" + std::to_string(iry));
+    *src_r = isy + ne;
+    *src_c = isx + ne;
+    *rec_r = iry + ne;
+    return TWI_OK;
+}
+
+LaunchShape default_shape(int rows_per_warp) {
+    return LaunchShape{rows_per_warp == 8 ? 8 : 4, 4};
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+
+struct twi_plan {
+    twi_problem p{};
+    int ne = 0, dimx = 0, dimz = 0, pitch = 0;
+    long long slot_elems = 0;
+    int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
+    bool gradient = true, kahan = true;
+    long long nslots = 0, nvirt = 0, nacc = 0;
+    // workspace regions (byte offsets)
+    size_t off_vel = 0, off_wav = 0, off_frd = 0, off_grad = 0, off_coords = 0, off_err = 0,
+           off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, total = 0;
+    char* ws = nullptr;
+    int device = -1;
+    CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
+    cudaGraphExec_t g_bwd = nullptr;
+    bool have_ckpt = false, have_shots = false, have_model = false;
+
+    float* F(size_t off) const { return reinterpret_cast<float*>(ws + off); }
+    int* I(size_t off) const { return reinterpret_cast<int*>(ws + off); }
+
+    Slot zero() const { return {0, 0}; }
+    Slot urot(int i) const { return {1 + i, sps}; }
+    Slot lrot(int i) const { return {4 + i, sps}; }
+    Slot ckpt(int j, int part) const { return {1 + 6 + 2 * (j - 1) + part, sps}; }
+
+    // slot of u^k during the forward pass
+    Slot fwd_slot(long long k, bool save) const {
+        if (k <= 0) return zero();
+        if (save && gradient) {
+            if (k % K == 0 && k / K < nseg) return ckpt((int)(k / K), 1);
+            if ((k + 1) % K == 0 && (k + 1) / K < nseg) return ckpt((int)((k + 1) / K), 0);
+        }
+        return urot((int)(k % 3));
+    }
+    // slot of u^k while recomputing segment j
+    Slot rec_slot(long long k, int j) const {
+        const long long c = (long long)j * K;
+        if (k <= c) return j == 0 ? zero() : ckpt(j, k == c ? 1 : 0);
+        return urot((int)(k % 3));
+    }
+    Slot lam_slot(long long m) const { return m < 0 ? zero() : lrot((int)(m % 3)); }
+
+    StepArgs base_args() const {
+        StepArgs a{};
+        a.dimx = dimx;
+        a.dimz = dimz;
+        a.pitch = pitch;
+        a.nx = p.nx;
+        a.nz = p.nz;
+        a.slot_elems = slot_elems;
+        a.fields = F(off_fields);
+        a.nshots = p.nshots;
+        a.spc = spc;
+        const float dt2 = p.dt * p.dt, h2 = p.h * p.h;
+        a.dt2 = dt2;
+        a.h2 = h2;
+        a.dtoh2 = dt2 / h2;
+        a.hdt = p.h * p.dt;
+        a.cons = static_cast<float>(-2.0 / static_cast<double>(dt2));
+        a.src_rc = I(off_coords);
+        a.rec_row = I(off_coords) + 2 * p.nshots;
+        a.wav = F(off_wav);
+        a.wav_stride = p.wavelet_per_shot ? p.nt : 0;
+        a.frd_stride = (long long)p.nt * p.nx;
+        a.resid_stride = (long long)p.nt * p.nx;
+        a.virt_slot_elems = slot_elems;
+        a.virt_pitch = pitch;
+        a.virt_vec4 = 1;
+        a.err = I(off_err);
+        return a;
+    }
+
+    int launch(StepMode mode, const StepArgs& a, cudaStream_t st) const {
+        cudaError_t e = launch_step(p.order, p.exact != 0, mode, default_shape(rz), tm_u2, tm_u1,
+                                    tm_vel, a, st);
+        if (e != cudaSuccess)
+            return fail(TWI_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+        return TWI_OK;
+    }
+
+    int enqueue_forward(bool save, cudaStream_t st) const {
+        StepArgs a = base_args();
+        a.frd = F(off_frd);
+        for (int it = 0; it < p.nt; ++it) {
+            const Slot pv = fwd_slot(it - 1, save), cu = fwd_slot(it, save),
+                       nx_ = fwd_slot(it + 1, save);
+            a.it = it;
+            a.prev_base = pv.base, a.prev_stride = pv.stride;
+            a.cur_base = cu.base, a.cur_stride = cu.stride;
+            a.next_base = nx_.base, a.next_stride = nx_.stride;
+            TWI_TRY(launch(kModeForward, a, st));
+        }
+        return TWI_OK;
+    }
+
+    int enqueue_gradient(cudaStream_t st) const {
+        const size_t acc_bytes = (size_t)nacc * slot_elems * 4;
+        if (cudaMemsetAsync(F(off_acc), 0, acc_bytes, st) != cudaSuccess ||
+            (kahan && cudaMemsetAsync(F(off_comp), 0, acc_bytes, st) != cudaSuccess))
+            return fail(TWI_ERR_CUDA, "memset of gradient accumulators failed");
+        StepArgs a = base_args();
+        a.virt_out = F(off_virt);
+        a.virt_in = F(off_virt);
+        a.virt_stride = K;
+        a.resid = F(off_frd);   // the resid region aliases the gathers region
+        a.acc = F(off_acc);
+        a.acc_comp = kahan ? F(off_comp) : nullptr;
+        a.acc_mode = kahan ? kAccKahanPerGroup : kAccPlainPerShot;
+        a.acc_base = 0;
+        for (int j = nseg - 1; j >= 0; --j) {
+            const int c0 = j * K;
+            const int L = std::min(K, p.nt - c0);
+            for (int it = c0; it < c0 + L; ++it) {     // recompute, writing virt
+                const Slot pv = rec_slot(it - 1, j), cu = rec_slot(it, j), nx_ = urot((it + 1) % 3);
+                a.it = it;
+                a.prev_base = pv.base, a.prev_stride = pv.stride;
+                a.cur_base = cu.base, a.cur_stride = cu.stride;
+                a.next_base = nx_.base, a.next_stride = nx_.stride;
+                a.virt_base = it - c0;
+                a.frd = nullptr;
+                TWI_TRY(launch(kModeRecompute, a, st));
+            }
+            for (int it = c0 + L - 1; it >= c0; --it) {  // adjoint, reading virt
+                const long long m = (long long)p.nt - 1 - it;
+                const Slot pv = lam_slot(m - 2), cu = lam_slot(m - 1), nx_ = lam_slot(m);
+                a.it = it;
+                a.prev_base = pv.base, a.prev_stride = pv.stride;
+                a.cur_base = cu.base, a.cur_stride = cu.stride;
+                a.next_base = nx_.base, a.next_stride = nx_.stride;
+                a.virt_base = it - c0;
+                TWI_TRY(launch(kModeAdjoint, a, st));
+            }
+        }
+        cudaError_t e = launch_reduce_grad(F(off_acc), kahan ? F(off_comp) : nullptr, (int)nacc,
+                                           slot_elems, pitch, ne, p.nx, p.nz, kahan ? 1 : 0,
+                                           F(off_grad), st);
+        if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("reduce: ") + cudaGetErrorString(e));
+        return TWI_OK;
+    }
+
+    void drop_graphs() {
+        for (auto& g : g_fwd)
+            if (g) cudaGraphExecDestroy(g), g = nullptr;
+        if (g_bwd) cudaGraphExecDestroy(g_bwd), g_bwd = nullptr;
+    }
+
+    // Run `enqueue` directly, or capture it once into a graph and replay.
+    template <typename Fn>
+    int run(cudaGraphExec_t* slot, cudaStream_t st, Fn enqueue) {
+        if (!p.use_graphs) return enqueue(st);
+        if (!*slot) {
+            if (!capture_stream)
+                TWI_CUDA(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
+            TWI_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+            int s = enqueue(capture_stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(capture_stream, &g);
+            if (s != TWI_OK) {
+                if (g) cudaGraphDestroy(g);
+                return s;
+            }
+            if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(slot, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+        }
+        TWI_CUDA(cudaGraphLaunch(*slot, st));
+        return TWI_OK;
+    }
+};
+
+extern "C" {
+
+int twi_version(void) { return 100; }
+
+const char* twi_last_error(void) { return g_last_error.c_str(); }
+
+int twi_plan_create(const twi_problem* prob, twi_plan** out) {
+    if (!prob || !out) return fail(TWI_ERR_INVALID, "null argument");
+    const twi_problem& p = *prob;
+    TWI_TRY(check_order(p.order));
+    if (p.nx < 1 || p.nz < 1 || p.nt < 1 || p.nshots < 1)
+        return fail(TWI_ERR_INVALID, "nx, nz, nt and nshots must be positive");
+    if (!(p.h > 0.f) || !(p.dt > 0.f)) return fail(TWI_ERR_INVALID, "h and dt must be positive");
+    if (p.rows_per_warp != 0 && p.rows_per_warp != 4 && p.rows_per_warp != 8)
+        return fail(TWI_ERR_INVALID, "rows_per_warp must be 0, 4 or 8");
+    if (p.ckpt_interval < 0 || p.ckpt_interval == 1)
+        return fail(TWI_ERR_INVALID, "ckpt_interval must be 0 (choose) or >= 2");
+
+    twi_plan* P = new twi_plan();
+    P->p = p;
+    P->ne = p.order / 2;
+    P->dimx = p.nx + p.order;
+    P->dimz = p.nz + p.order;
+    P->pitch = (P->dimx + kTileX - 1) / kTileX * kTileX;
+    P->slot_elems = (long long)P->pitch * P->dimz;
+    P->gradient = p.ckpt_interval >= 0;   // all plans can take gradients
+    P->kahan = p.accumulate == 0;
+    P->rz = p.rows_per_warp ? p.rows_per_warp : 4;
+    int K = p.ckpt_interval;
+    if (K == 0) K = std::max(2, (int)std::lround(std::sqrt(2.0 * p.nt)));
+    K = std::min(K, std::max(2, p.nt));
+    P->K = K;
+    P->nseg = (p.nt + K - 1) / K;
+    int spc = p.shots_per_cta;
+    if (spc <= 0) spc = std::min(p.nshots, 4);
+    P->spc = std::min(spc, p.nshots);
+    P->ngroups = (p.nshots + P->spc - 1) / P->spc;
+    P->sps = 6 + 2 * (P->nseg - 1);
+    P->nslots = 1 + (long long)p.nshots * P->sps;
+    P->nvirt = (long long)p.nshots * K;
+    P->nacc = P->kahan ? P->ngroups : p.nshots;
+
+    // workspace layout
+    const size_t S = p.nshots, nt = p.nt;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
+    P->off_vel = take((size_t)p.nx * p.nz * 4);
+    P->off_wav = take((p.wavelet_per_shot ? S : 1) * nt * 4);
+    P->off_frd = take(S * nt * p.nx * 4);
+    P->off_grad = take((size_t)p.nx * p.nz * 4);
+    P->off_coords = take(S * 3 * 4);
+    P->off_err = take(4);
+    P->off_vpad = take((size_t)P->slot_elems * 4);
+    P->off_fields = take((size_t)P->nslots * P->slot_elems * 4);
+    P->off_virt = take((size_t)P->nvirt * P->slot_elems * 4);
+    P->off_acc = take((size_t)P->nacc * P->slot_elems * 4);
+    P->off_comp = take(P->kahan ? (size_t)P->nacc * P->slot_elems * 4 : 0);
+    P->total = off;
+    *out = P;
+    return TWI_OK;
+}
+
+int twi_plan_layout(const twi_plan* P, twi_layout* out) {
+    if (!P || !out) return fail(TWI_ERR_INVALID, "null argument");
+    out->workspace_bytes = P->total;
+    out->vel = P->off_vel;
+    out->wavelet = P->off_wav;
+    out->gathers = P->off_frd;
+    out->resid = P->off_frd;
+    out->grad = P->off_grad;
+    out->dimx = P->dimx;
+    out->dimz = P->dimz;
+    out->pitch = P->pitch;
+    out->ckpt_interval = P->K;
+    out->nsegments = P->nseg;
+    out->shots_per_cta = P->spc;
+    out->rows_per_warp = P->rz;
+    return TWI_OK;
+}
+
+int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
+    if (!P || !workspace) return fail(TWI_ERR_INVALID, "null argument");
+    if (bytes < P->total)
+        return fail(TWI_ERR_NOMEM, "workspace too small: need " + std::to_string(P->total) + " bytes");
+    if (reinterpret_cast<uintptr_t>(workspace) % 256)
+        return fail(TWI_ERR_INVALID, "workspace must be 256-byte aligned");
+    P->drop_graphs();
+    P->ws = static_cast<char*>(workspace);
+    TWI_CUDA(cudaGetDevice(&P->device));
+    TWI_CUDA(prepare_step(P->p.order, P->p.exact != 0, default_shape(P->rz)));
+    const int HZ = zhalo(P->p.order);
+    const int TZ = P->rz * 4;
+    TWI_TRY(make_map(&P->tm_u2, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kBoxX,
+                     TZ + 2 * HZ));
+    TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kBoxX,
+                     TZ + 1));
+    TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
+    // zero slot, error word and velocity padding columns
+    TWI_CUDA(cudaMemset(P->F(P->off_fields), 0, (size_t)P->slot_elems * 4));
+    TWI_CUDA(cudaMemset(P->I(P->off_err), 0, 4));
+    TWI_CUDA(cudaMemset(P->F(P->off_vpad), 0, (size_t)P->slot_elems * 4));
+    P->have_ckpt = false;
+    return TWI_OK;
+}
+
+int twi_plan_set_shots(twi_plan* P, const float* sx, const float* sy, const float* ry,
+                       void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!sx || !sy || !ry) return fail(TWI_ERR_INVALID, "null coordinate array");
+    const int S = P->p.nshots;
+    std::vector<int> c(3 * S);
+    for (int s = 0; s < S; ++s) {
+        int r, cc, rr;
+        int st = shot_cells(sx[s], sy[s], ry[s], P->p.h, P->p.nx, P->p.nz, P->ne, P->dimz, &r, &cc, &rr);
+        if (st != TWI_OK) return fail(st, "shot " + std::to_string(s) + ": " + g_last_error);
+        c[2 * s] = r;
+        c[2 * s + 1] = cc;
+        c[2 * S + s] = rr;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TWI_CUDA(cudaMemcpyAsync(P->I(P->off_coords), c.data(), c.size() * 4, cudaMemcpyHostToDevice, st));
+    TWI_CUDA(cudaStreamSynchronize(st));   // the host vector goes out of scope
+    P->have_shots = true;
+    P->have_ckpt = false;
+    return TWI_OK;
+}
+
+int twi_plan_set_model(twi_plan* P, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    cudaError_t e = launch_pad_model(P->F(P->off_vel), P->F(P->off_vpad), P->p.nx, P->p.nz, P->ne,
+                                     P->dimx, P->dimz, P->pitch, static_cast<cudaStream_t>(stream));
+    if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("pad: ") + cudaGetErrorString(e));
+    P->have_model = true;
+    P->have_ckpt = false;
+    return TWI_OK;
+}
+
+int twi_forward(twi_plan* P, int save_checkpoints, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!P->have_shots || !P->have_model)
+        return fail(TWI_ERR_STATE, "set shots and model before twi_forward");
+    const bool save = save_checkpoints != 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TWI_TRY(P->run(&P->g_fwd[save ? 1 : 0], st,
+                   [&](cudaStream_t s) { return P->enqueue_forward(save, s); }));
+    P->have_ckpt = save;
+    return TWI_OK;
+}
+
+int twi_gradient(twi_plan* P, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!P->have_ckpt)
+        return fail(TWI_ERR_STATE, "twi_gradient needs a preceding twi_forward(save_checkpoints=1)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return P->run(&P->g_bwd, st, [&](cudaStream_t s) { return P->enqueue_gradient(s); });
+}
+
+int twi_plan_check(twi_plan* P, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    int err = 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TWI_CUDA(cudaMemcpyAsync(&err, P->I(P->off_err), 4, cudaMemcpyDeviceToHost, st));
+    TWI_CUDA(cudaStreamSynchronize(st));
+    if (err) {
+        cudaMemsetAsync(P->I(P->off_err), 0, 4, st);
+        return fail(TWI_ERR_DEVICE, "device error word " + std::to_string(err) +
+                                        " (a bounded TMA wait ran out)");
+    }
+    return TWI_OK;
+}
+
+int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!ms_per_launch || repeats < 1 || mode < 0 || mode > 2)
+        return fail(TWI_ERR_INVALID, "mode must be 0, 1 or 2 and repeats >= 1");
+    if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    StepArgs a = P->base_args();
+    const int it = P->p.nt / 2;
+    a.it = it;
+    const StepMode m = static_cast<StepMode>(mode);
+    if (m == kModeAdjoint) {
+        a.prev_base = 4, a.cur_base = 5, a.next_base = 6;   // adjoint rotation
+        a.virt_in = P->F(P->off_virt);
+        a.resid = P->F(P->off_frd);
+        a.acc = P->F(P->off_acc);
+        a.acc_comp = P->kahan ? P->F(P->off_comp) : nullptr;
+        a.acc_mode = P->kahan ? kAccKahanPerGroup : kAccPlainPerShot;
+    } else {
+        a.prev_base = 1, a.cur_base = 2, a.next_base = 3;   // forward rotation
+        if (m == kModeRecompute) a.virt_out = P->F(P->off_virt);
+    }
+    a.prev_stride = a.cur_stride = a.next_stride = P->sps;
+    a.virt_stride = P->K;
+    a.virt_base = 0;
+    cudaEvent_t e0, e1;
+    TWI_CUDA(cudaEventCreate(&e0));
+    TWI_CUDA(cudaEventCreate(&e1));
+    int s = TWI_OK;
+    if (cudaEventRecord(e0, st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event record failed");
+    for (int r = 0; r < repeats && s == TWI_OK; ++r) s = P->launch(m, a, st);
+    if (s == TWI_OK && cudaEventRecord(e1, st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event record failed");
+    if (s == TWI_OK && cudaEventSynchronize(e1) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event sync failed");
+    float ms = 0.f;
+    if (s == TWI_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) s = fail(TWI_ERR_CUDA, "elapsed failed");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s == TWI_OK) *ms_per_launch = ms / repeats;
+    return s;
+}
+
+int twi_plan_destroy(twi_plan* P) {
+    if (!P) return TWI_OK;
+    P->drop_graphs();
+    if (P->capture_stream) cudaStreamDestroy(P->capture_stream);
+    delete P;
+    return TWI_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// reference-shaped entry points (single shot, reference memory layout)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct RefRun {
+    int order, ne, dimx, dimz, nx, nz, nt, pitch;
+    long long slot_elems;
+    float h, dt;
+    char* scratch = nullptr;
+    size_t off_vpad = 0, off_fields = 0, off_wav = 0, off_coords = 0, off_err = 0, off_acc = 0,
+           total = 0;
+    CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
+    cudaStream_t st = nullptr;
+
+    float* F(size_t o) const { return reinterpret_cast<float*>(scratch + o); }
+    int* I(size_t o) const { return reinterpret_cast<int*>(scratch + o); }
+
+    int setup(int order_, int dimx_, int dimy_, int nt_, float h_, float dt_, bool with_acc,
+              cudaStream_t st_) {
+        TWI_TRY(check_order(order_));
+        order = order_, ne = order_ / 2, dimx = dimx_, dimz = dimy_, nt = nt_, h = h_, dt = dt_;
+        nx = dimx - order;
+        nz = dimz - order;
+        st = st_;
+        if (nx < 1 || nz < 1 || nt < 1) return fail(TWI_ERR_INVALID, "dimx, dimy must exceed order and nt >= 1");
+        if (!(h > 0.f) || !(dt > 0.f)) return fail(TWI_ERR_INVALID, "h and dt must be positive");
+        pitch = (dimx + kTileX - 1) / kTileX * kTileX;
+        slot_elems = (long long)pitch * dimz;
+        size_t off = 0;
+        auto take = [&](size_t b) { size_t o = off; off = align256(off + b); return o; };
+        off_vpad = take((size_t)slot_elems * 4);
+        off_fields = take((size_t)4 * slot_elems * 4);   // zero slot + 3 rotating
+        off_acc = take(with_acc ? (size_t)slot_elems * 4 : 0);
+        off_wav = take((size_t)nt * 4);
+        off_coords = take(3 * 4);
+        off_err = take(4);
+        total = off;
+        void* p = nullptr;
+        TWI_CUDA(cudaMallocAsync(&p, total, st));
+        scratch = static_cast<char*>(p);
+        TWI_CUDA(cudaMemsetAsync(scratch, 0, total, st));
+        TWI_CUDA(prepare_step(order, true, LaunchShape{4, 4}));
+        const int TZ = 16, HZ = zhalo(order);
+        TWI_TRY(make_map(&tm_u2, F(off_fields), dimx, dimz, 4, pitch, kBoxX, TZ + 2 * HZ));
+        TWI_TRY(make_map(&tm_u1, F(off_fields), dimx, dimz, 4, pitch, kBoxX, TZ + 1));
+        TWI_TRY(make_map(&tm_vel, F(off_vpad), dimx, dimz, 0, pitch, kTileX, TZ));
+        return TWI_OK;
+    }
+
+    int load_vel(const float* vel) {
+        TWI_CUDA(cudaMemcpy2DAsync(F(off_vpad), (size_t)pitch * 4, vel, (size_t)dimx * 4,
+                                   (size_t)dimx * 4, dimz, cudaMemcpyDeviceToDevice, st));
+        return TWI_OK;
+    }
+
+    StepArgs args() const {
+        StepArgs a{};
+        a.dimx = dimx, a.dimz = dimz, a.pitch = pitch, a.nx = nx, a.nz = nz;
+        a.slot_elems = slot_elems;
+        a.fields = F(off_fields);
+        a.nshots = 1;
+        a.spc = 1;
+        const float dt2 = dt * dt, h2 = h * h;
+        a.dt2 = dt2, a.h2 = h2, a.dtoh2 = dt2 / h2, a.hdt = h * dt;
+        a.cons = static_cast<float>(-2.0 / static_cast<double>(dt2));
+        a.src_rc = I(off_coords);
+        a.rec_row = I(off_coords) + 2;
+        a.wav = F(off_wav);
+        a.wav_stride = 0;
+        a.frd_stride = (long long)nt * nx;
+        a.resid_stride = (long long)nt * nx;
+        a.err = I(off_err);
+        return a;
+    }
+
+    int launch(StepMode mode, const StepArgs& a) const {
+        cudaError_t e = launch_step(order, true, mode, LaunchShape{4, 4}, tm_u2, tm_u1, tm_vel, a, st);
+        if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+        return TWI_OK;
+    }
+
+    // read the error word, release scratch
+    int finish(int status) {
+        int err = 0;
+        if (scratch) {
+            if (status == TWI_OK) {
+                if (cudaMemcpyAsync(&err, I(off_err), 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                    status = fail(TWI_ERR_CUDA, "error word copy failed");
+            }
+            cudaFreeAsync(scratch, st);
+            scratch = nullptr;
+            if (cudaStreamSynchronize(st) != cudaSuccess && status == TWI_OK)
+                status = fail(TWI_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
+        }
+        if (status == TWI_OK && err)
+            status = fail(TWI_ERR_DEVICE, "device error word " + std::to_string(err));
+        return status;
+    }
+};
+
+Slot rot_slot(long long k) { return k <= 0 ? Slot{0, 0} : Slot{1 + (int)(k % 3), 0}; }
+
+int ref_forward(float* frd, float* virt, const float* vel, const float* w, int order, int dimx,
+                int dimy, int nt, float h, float dt, float sx, float sy, float ry,
+                cudaStream_t st) {
+    if (!frd || !vel || !w) return fail(TWI_ERR_INVALID, "null array");
+    RefRun R;
+    int s = R.setup(order, dimx, dimy, nt, h, dt, false, st);
+    if (s == TWI_OK) s = R.load_vel(vel);
+    int coords[3];
+    if (s == TWI_OK) s = shot_cells(sx, sy, ry, h, R.nx, R.nz, R.ne, R.dimz, &coords[0], &coords[1], &coords[2]);
+    if (s == TWI_OK && cudaMemcpyAsync(R.I(R.off_coords), coords, 12, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "coordinate upload failed");
+    if (s == TWI_OK && cudaMemcpyAsync(R.F(R.off_wav), w, (size_t)nt * 4, cudaMemcpyDefault, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "wavelet upload failed");
+    if (s == TWI_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "sync failed");
+    if (s == TWI_OK) {
+        StepArgs a = R.args();
+        a.frd = frd;
+        a.virt_out = virt;
+        a.virt_slot_elems = (long long)dimx * dimy;
+        a.virt_pitch = dimx;
+        a.virt_stride = 0;
+        a.virt_vec4 = (dimx % 4 == 0 && reinterpret_cast<uintptr_t>(virt) % 16 == 0) ? 1 : 0;
+        for (int it = 0; it < nt && s == TWI_OK; ++it) {
+            const Slot pv = rot_slot(it - 1), cu = rot_slot(it), nx_ = rot_slot(it + 1);
+            a.it = it;
+            a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
+            a.virt_base = it;
+            s = R.launch(virt ? kModeRecompute : kModeForward, a);
+        }
+    }
+    return R.finish(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int twi_fdm_forward(float* frd, float* virt, float* u1, float* u2, float* u3, const float* vel,
+                    const float* w, int order, int dimx, int dimy, int nt, float h, float dt,
+                    float sx, float sy, float ry, void* stream) {
+    (void)u1, (void)u2, (void)u3;
+    if (!virt) return fail(TWI_ERR_INVALID, "virt must not be null (use twi_fdm_forward_only)");
+    return ref_forward(frd, virt, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int twi_fdm_forward_only(float* frd, float* u1, float* u2, float* u3, const float* vel,
+                         const float* w, int order, int dimx, int dimy, int nt, float h,
+                         float dt, float sx, float sy, float ry, void* stream) {
+    (void)u1, (void)u2, (void)u3;
+    return ref_forward(frd, nullptr, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
+                       static_cast<cudaStream_t>(stream));
+}
+
+int twi_fdm_backward(float* grad, const float* virt, float* u1, float* u2, float* u3,
+                     const float* vel, const float* resid, int order, int dimx, int dimy, int nt,
+                     float h, float dt, float ry, void* stream) {
+    (void)u1, (void)u2, (void)u3;
+    if (!grad || !virt || !vel || !resid) return fail(TWI_ERR_INVALID, "null array");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RefRun R;
+    int s = R.setup(order, dimx, dimy, nt, h, dt, true, st);
+    if (s == TWI_OK) s = R.load_vel(vel);
+    int coords[3] = {-1, -1, 0};
+    if (s == TWI_OK) {
+        const int iry = cell_of(ry, h);
+        if (!(ry >= 0.f) || iry + R.ne >= R.dimz)
+            s = fail(TWI_ERR_INVALID, "receiver row outside the grid: iry=" + std::to_string(iry));
+        coords[2] = iry + R.ne;
+    }
+    if (s == TWI_OK && cudaMemcpyAsync(R.I(R.off_coords), coords, 12, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "coordinate upload failed");
+    if (s == TWI_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "sync failed");
+    if (s == TWI_OK) {
+        StepArgs a = R.args();
+        a.resid = resid;
+        a.virt_in = virt;
+        a.virt_slot_elems = (long long)dimx * dimy;
+        a.virt_pitch = dimx;
+        a.virt_stride = 0;
+        a.virt_vec4 = (dimx % 4 == 0 && reinterpret_cast<uintptr_t>(virt) % 16 == 0) ? 1 : 0;
+        a.acc = R.F(R.off_acc);
+        a.acc_mode = kAccPlainPerShot;
+        a.acc_base = 0;
+        for (int it = nt - 1; it >= 0 && s == TWI_OK; --it) {
+            const long long m = (long long)nt - 1 - it;
+            const Slot pv = rot_slot(m - 1), cu = rot_slot(m), nx_ = rot_slot(m + 1);
+            a.it = it;
+            a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
+            a.virt_base = it;
+            s = R.launch(kModeAdjoint, a);
+        }
+        if (s == TWI_OK &&
+            cudaMemcpy2DAsync(grad, (size_t)dimx * 4, R.F(R.off_acc), (size_t)R.pitch * 4,
+                              (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            s = fail(TWI_ERR_CUDA, "gradient copy failed");
+    }
+    return R.finish(s);
+}
+
+}  // extern "C"

@@ -1,0 +1,561 @@
+// twi_step.cu -- the fused time-step kernel and its small helpers.
+//
+// One launch advances every shot of a batch by one time step.  A CTA owns a
+// 128-column x TZ-row tile of the padded grid and a group of `spc` shots
+// that share the velocity tile.  For each shot it stages u^n (with a 4-column
+// / HZ-row halo) and u^{n-1} (4-column / 1-row halo) into shared memory with
+// TMA, double-buffered across shots, and computes in one pass what the
+// reference does with five launches and a memcpy per step
+// (propagator_cpu.cpp:57-78, propagator_cuda.cu:61-80):
+//   * the interior leapfrog update (orders 2/4/8),
+//   * the Keys absorbing update of the left/right/bottom pads,
+//   * the point source (forward) or the adjoint source on the receiver row,
+//   * the receiver-row gather (forward),
+//   * the virtual source -2/(v^3 dt^2) (u^{n+1} - 2u^n + u^{n-1}) (recompute),
+//   * the gradient term -virt * lambda with Kahan or plain accumulation
+//     (adjoint).
+// Each warp streams RZ consecutive rows: a (2*NE+1)-row register window of
+// float4s along z, and warp shuffles for the x neighbours (lanes 0 and 31
+// read the x halo from shared memory).  Rows/columns of the pads use the
+// general per-cell path.  The top NE rows are the free surface: always 0.
+#include <cstdio>
+
+#include "twi_cell.cuh"
+#include "twi_kernels.h"
+#include "twi_ptx.cuh"
+
+namespace twi {
+namespace {
+
+constexpr int round32(int n) { return (n + 31) / 32 * 32; }
+
+template <int ORDER, int RZ, int WZ>
+struct Smem {
+    static constexpr int NE = ORDER / 2;
+    static constexpr int TZ = RZ * WZ;
+    static constexpr int HZ = zhalo(ORDER);
+    static constexpr int U2_ROWS = TZ + 2 * HZ;
+    static constexpr int U1_ROWS = TZ + 1;
+    static constexpr int U2_FLOATS = round32(U2_ROWS * kBoxX);
+    static constexpr int U1_FLOATS = round32(U1_ROWS * kBoxX);
+    static constexpr int STAGE_FLOATS = U2_FLOATS + U1_FLOATS;
+    static constexpr int V_FLOATS = TZ * kTileX;
+    static constexpr int STAGES = 2;
+    static constexpr int BAR_BYTES = 128;
+    static constexpr size_t BYTES =
+        128 /*alignment slack*/ + BAR_BYTES + size_t(V_FLOATS + STAGES * STAGE_FLOATS) * 4;
+    static constexpr uint32_t U2_TX = U2_ROWS * kBoxX * 4;
+    static constexpr uint32_t U1_TX = U1_ROWS * kBoxX * 4;
+    static constexpr uint32_t V_TX = TZ * kTileX * 4;
+};
+
+__device__ __forceinline__ float comp(const float4& v, int m) {
+    return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void set_comp(float4& v, int m, float x) {
+    if (m == 0) v.x = x;
+    else if (m == 1) v.y = x;
+    else if (m == 2) v.z = x;
+    else v.w = x;
+}
+__device__ __forceinline__ float4 ld4(const float* p) {
+    return *reinterpret_cast<const float4*>(p);
+}
+
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32)
+step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
+            const __grid_constant__ CUtensorMap tm_vel, const StepArgs a) {
+    using S = Smem<ORDER, RZ, WZ>;
+    constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
+
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* sbase = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sbase);  // [0] velocity, [1+i] stage i
+    float* vs = reinterpret_cast<float*>(sbase + S::BAR_BYTES);
+    float* stage0 = vs + S::V_FLOATS;
+
+    const int x0 = blockIdx.x * kTileX;
+    const int z0 = blockIdx.y * TZ;
+    const int s_begin = blockIdx.z * a.spc;
+    const int nloc = min(a.spc, a.nshots - s_begin);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (nloc <= 0) return;
+
+    if (threadIdx.x == 0) {
+        prefetch_tmap(&tm_u2);
+        prefetch_tmap(&tm_u1);
+        prefetch_tmap(&tm_vel);
+#pragma unroll
+        for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    auto issue = [&](int k) {
+        const int s = s_begin + k;
+        float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
+        uint64_t* b = &bar[1 + (k % STAGES)];
+        mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
+        tma_load_3d(st, &tm_u2, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
+        tma_load_3d(st + S::U2_FLOATS, &tm_u1, x0 - kHaloX, z0 - 1,
+                    a.prev_base + s * a.prev_stride, b);
+    };
+    if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bar[0], S::V_TX);
+        tma_load_2d(vs, &tm_vel, x0, z0, &bar[0]);
+        for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+    }
+
+    const int rl0 = warp * RZ;           // first tile-local row of this warp
+    const int c = x0 + 4 * lane;         // first column of this lane
+    const int cs = kHaloX + 4 * lane;    // its shared-memory column
+
+    // -- velocity tile: kept in registers for all shots --------------------------
+    {
+        const bool ok = mbar_wait_bounded(&bar[0], 0);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(a.err, 1);
+            return;
+        }
+    }
+    float4 vreg[RZ], vvreg[RZ];
+#pragma unroll
+    for (int rr = 0; rr < RZ; ++rr) {
+        vreg[rr] = ld4(vs + (rl0 + rr) * kTileX + 4 * lane);
+        vvreg[rr] = make_float4(vv_of<EXACT>(vreg[rr].x, a.dtoh2), vv_of<EXACT>(vreg[rr].y, a.dtoh2),
+                                vv_of<EXACT>(vreg[rr].z, a.dtoh2), vv_of<EXACT>(vreg[rr].w, a.dtoh2));
+    }
+
+    // -- Kahan accumulators of this CTA's shot group (adjoint) -----------------------
+    float4 gsum[MODE == kModeAdjoint ? RZ : 1], gcmp[MODE == kModeAdjoint ? RZ : 1];
+    const bool col_ok = c < a.dimx;
+    if constexpr (MODE == kModeAdjoint) {
+        if (a.acc_mode == kAccKahanPerGroup) {
+            const long long slot = a.acc_base + blockIdx.z;
+#pragma unroll
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int r = z0 + rl0 + rr;
+                gsum[rr] = gcmp[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (col_ok && r < a.dimz) {
+                    const long long off = slot * a.slot_elems + (long long)r * a.pitch + c;
+                    gsum[rr] = ld4(a.acc + off);
+                    gcmp[rr] = ld4(a.acc_comp + off);
+                }
+            }
+        }
+    }
+
+    for (int k = 0; k < nloc; ++k) {
+        const int s = s_begin + k;
+        const float* u2s = stage0 + (k % STAGES) * S::STAGE_FLOATS;
+        const float* u1s = u2s + S::U2_FLOATS;
+
+        int src_r = -1, src_c = -1;
+        float wamp = 0.f;
+        if constexpr (MODE != kModeAdjoint) {
+            src_r = a.src_rc[2 * s];
+            src_c = a.src_rc[2 * s + 1];
+            wamp = a.wav[(long long)s * a.wav_stride + a.it];
+        }
+        const int rec_r = a.rec_row[s];
+
+        // virtual source of this step for the warp's rows (adjoint)
+        float4 vin[MODE == kModeAdjoint ? RZ : 1];
+        if constexpr (MODE == kModeAdjoint) {
+            const float* vbase = a.virt_in + (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems;
+#pragma unroll
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int r = z0 + rl0 + rr;
+                vin[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (col_ok && r < a.dimz) {
+                    const float* p = vbase + (long long)r * a.virt_pitch + c;
+                    if (a.virt_vec4) {
+                        vin[rr] = ld4(p);
+                    } else {
+                        vin[rr].x = p[0];
+                        if (c + 1 < a.dimx) vin[rr].y = p[1];
+                        if (c + 2 < a.dimx) vin[rr].z = p[2];
+                        if (c + 3 < a.dimx) vin[rr].w = p[3];
+                    }
+                }
+            }
+        }
+
+        {
+            const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicOr(a.err, 1);
+                return;
+            }
+        }
+
+        float4 win[2 * NE + 1];
+#pragma unroll
+        for (int j = 0; j < 2 * NE; ++j) win[j] = ld4(u2s + (rl0 + HZ - NE + j) * kBoxX + cs);
+
+#pragma unroll
+        for (int rr = 0; rr < RZ; ++rr) {
+            const int rl = rl0 + rr;
+            const int r = z0 + rl;
+            win[2 * NE] = ld4(u2s + (rl + HZ + NE) * kBoxX + cs);
+            const float c4[4] = {win[NE].x, win[NE].y, win[NE].z, win[NE].w};
+            float L[NE], Rr[NE];   // L[k]: column c-1-k, Rr[k]: column c+4+k
+#pragma unroll
+            for (int kk = 0; kk < NE; ++kk) {
+                L[kk] = __shfl_up_sync(0xffffffffu, c4[3 - kk], 1);
+                Rr[kk] = __shfl_down_sync(0xffffffffu, c4[kk], 1);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int kk = 0; kk < NE; ++kk) L[kk] = u2s[(rl + HZ) * kBoxX + cs - 1 - kk];
+            }
+            if (lane == 31) {
+#pragma unroll
+                for (int kk = 0; kk < NE; ++kk) Rr[kk] = u2s[(rl + HZ) * kBoxX + cs + 4 + kk];
+            }
+            const float4 um4 = ld4(u1s + (rl + 1) * kBoxX + cs);
+            const float um[4] = {um4.x, um4.y, um4.z, um4.w};
+
+            const bool row_ok = r < a.dimz;
+            const bool interior_row = r >= NE && r < a.dimz - NE;
+            const bool fast = interior_row && c >= NE && c + 3 < a.dimx - NE;
+            float out[4];
+            if (fast) {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    float lf[NE], rt[NE], up[NE], dn[NE];
+#pragma unroll
+                    for (int d = 1; d <= NE; ++d) {
+                        const int jl = m - d, jr = m + d;
+                        lf[d - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
+                        rt[d - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
+                        up[d - 1] = comp(win[NE - d], m);
+                        dn[d - 1] = comp(win[NE + d], m);
+                    }
+                    out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], um[m],
+                                                           comp(vvreg[rr], m));
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < 4; ++m) {
+                    const int cc = c + m;
+                    out[m] = 0.f;
+                    if (row_ok && cc < a.dimx && r >= NE) {
+                        const float* U2 = u2s + (rl + HZ) * kBoxX + cs + m;
+                        const float* U1 = u1s + (rl + 1) * kBoxX + cs + m;
+                        const float v = comp(vreg[rr], m);
+                        if (r >= a.dimz - NE) {          // bottom pad (all columns)
+                            out[m] = keys_cell<EXACT>(U2[0], U2[-kBoxX], U2[-2 * kBoxX], U1[0],
+                                                      U1[-kBoxX], v, a.h2, a.dt2, a.hdt);
+                        } else if (cc < NE) {            // left pad
+                            out[m] = keys_cell<EXACT>(U2[0], U2[1], U2[2], U1[0], U1[1], v, a.h2,
+                                                      a.dt2, a.hdt);
+                        } else if (cc >= a.dimx - NE) {  // right pad
+                            out[m] = keys_cell<EXACT>(U2[0], U2[-1], U2[-2], U1[0], U1[-1], v,
+                                                      a.h2, a.dt2, a.hdt);
+                        } else {                          // interior
+                            float lf[NE], rt[NE], up[NE], dn[NE];
+#pragma unroll
+                            for (int d = 1; d <= NE; ++d) {
+                                lf[d - 1] = U2[-d];
+                                rt[d - 1] = U2[d];
+                                up[d - 1] = U2[-d * kBoxX];
+                                dn[d - 1] = U2[d * kBoxX];
+                            }
+                            out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, U2[0], U1[0],
+                                                                   comp(vvreg[rr], m));
+                        }
+                    }
+                }
+            }
+
+            // sources: only cells updated by the interior stencil receive them
+            // (the reference adds before Keys, which overwrites pad cells).
+            if constexpr (MODE != kModeAdjoint) {
+                if (r == src_r && interior_row) {
+#pragma unroll
+                    for (int m = 0; m < 4; ++m)
+                        if (c + m == src_c && src_c >= NE && src_c < a.dimx - NE)
+                            out[m] = add_injection<EXACT>(out[m], wamp, comp(vreg[rr], m), a.dt2);
+                }
+            } else {
+                if (r == rec_r && interior_row) {
+                    const float* rs = a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int cc = c + m;
+                        if (cc >= NE && cc < NE + a.nx)
+                            out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(vreg[rr], m), a.dt2);
+                    }
+                }
+            }
+
+            if (row_ok && col_ok) {
+                float* dst = a.fields + (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
+                             (long long)r * a.pitch + c;
+                *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+            }
+
+            if constexpr (MODE != kModeAdjoint) {
+                if (a.frd != nullptr && r == rec_r) {
+                    float* g = a.frd + (long long)s * a.frd_stride + (long long)a.it * a.nx;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int cc = c + m;
+                        if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                    }
+                }
+            }
+
+            if constexpr (MODE == kModeRecompute) {
+                if (row_ok && col_ok) {
+                    float vo[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int cc = c + m;
+                        // every grid cell, as the reference stores it (pads included)
+                        vo[m] = cc < a.dimx
+                                    ? virt_of<EXACT>(um[m], c4[m], out[m], comp(vreg[rr], m), a.cons)
+                                    : 0.f;
+                    }
+                    float* p = a.virt_out +
+                               (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                               (long long)r * a.virt_pitch + c;
+                    if (a.virt_vec4) {
+                        *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
+                    } else {
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m < a.dimx) p[m] = vo[m];
+                    }
+                }
+            }
+
+            if constexpr (MODE == kModeAdjoint) {
+                // every grid cell, as the reference accumulates it; callers
+                // crop the model region
+                if (row_ok && col_ok) {
+                    if (a.acc_mode == kAccKahanPerGroup) {
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const int cc = c + m;
+                            if (cc < a.dimx) {
+                                float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                                kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                set_comp(gsum[rr], m, sm);
+                                set_comp(gcmp[rr], m, cm);
+                            }
+                        }
+                    } else if (a.acc_mode == kAccPlainPerShot) {
+                        float4* g = reinterpret_cast<float4*>(
+                            a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                            (long long)r * a.pitch + c);
+                        float4 gv = *g;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const int cc = c + m;
+                            if (cc < a.dimx)
+                                set_comp(gv, m, __fadd_rn(comp(gv, m),
+                                                          grad_term<EXACT>(comp(vin[rr], m), out[m])));
+                        }
+                        *g = gv;
+                    }
+                }
+            }
+
+#pragma unroll
+            for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
+        }
+
+        __syncthreads();   // every warp is done with this stage
+        if (threadIdx.x == 0 && k + STAGES < nloc) issue(k + STAGES);
+    }
+
+    if constexpr (MODE == kModeAdjoint) {
+        if (a.acc_mode == kAccKahanPerGroup) {
+            const long long slot = a.acc_base + blockIdx.z;
+#pragma unroll
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int r = z0 + rl0 + rr;
+                if (col_ok && r < a.dimz) {
+                    const long long off = slot * a.slot_elems + (long long)r * a.pitch + c;
+                    *reinterpret_cast<float4*>(a.acc + off) = gsum[rr];
+                    *reinterpret_cast<float4*>(a.acc_comp + off) = gcmp[rr];
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch dispatch
+// ---------------------------------------------------------------------------
+
+// Set the dynamic shared-memory limit of one instantiation on the current
+// device (once per device; done before any stream capture).
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+cudaError_t configure_one() {
+    using S = Smem<ORDER, RZ, WZ>;
+    static unsigned long long configured = 0;   // one bit per device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64 || (configured & (1ull << dev))) return cudaSuccess;
+    e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+    if (e == cudaSuccess) configured |= 1ull << dev;
+    return e;
+}
+
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+cudaError_t launch_one(const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
+                       const CUtensorMap& tm_vel, const StepArgs* a, cudaStream_t stream) {
+    using S = Smem<ORDER, RZ, WZ>;
+    cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
+    if (e != cudaSuccess || a == nullptr) return e;
+    auto kern = step_kernel<ORDER, EXACT, MODE, RZ, WZ>;
+    dim3 grid((a->dimx + kTileX - 1) / kTileX, (a->dimz + S::TZ - 1) / S::TZ,
+              (a->nshots + a->spc - 1) / a->spc);
+    kern<<<grid, WZ * 32, S::BYTES, stream>>>(tm_u2, tm_u1, tm_vel, *a);
+    return cudaGetLastError();
+}
+
+template <int ORDER, bool EXACT, int MODE>
+cudaError_t launch_shape(LaunchShape sh, const CUtensorMap& t2, const CUtensorMap& t1,
+                         const CUtensorMap& tv, const StepArgs* a, cudaStream_t st) {
+    if (sh.warps == 4 && sh.rows_per_warp == 4) return launch_one<ORDER, EXACT, MODE, 4, 4>(t2, t1, tv, a, st);
+    if (sh.warps == 4 && sh.rows_per_warp == 8) return launch_one<ORDER, EXACT, MODE, 8, 4>(t2, t1, tv, a, st);
+    return cudaErrorInvalidValue;
+}
+
+template <int ORDER, bool EXACT>
+cudaError_t launch_mode(StepMode mode, LaunchShape sh, const CUtensorMap& t2,
+                        const CUtensorMap& t1, const CUtensorMap& tv, const StepArgs* a,
+                        cudaStream_t st) {
+    switch (mode) {
+        case kModeForward: return launch_shape<ORDER, EXACT, kModeForward>(sh, t2, t1, tv, a, st);
+        case kModeRecompute: return launch_shape<ORDER, EXACT, kModeRecompute>(sh, t2, t1, tv, a, st);
+        case kModeAdjoint: return launch_shape<ORDER, EXACT, kModeAdjoint>(sh, t2, t1, tv, a, st);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <int ORDER>
+cudaError_t launch_arith(bool exact, StepMode mode, LaunchShape sh, const CUtensorMap& t2,
+                         const CUtensorMap& t1, const CUtensorMap& tv, const StepArgs* a,
+                         cudaStream_t st) {
+    return exact ? launch_mode<ORDER, true>(mode, sh, t2, t1, tv, a, st)
+                 : launch_mode<ORDER, false>(mode, sh, t2, t1, tv, a, st);
+}
+
+// ---------------------------------------------------------------------------
+// model padding and gradient reduction (32x32 shared-memory transposes)
+// ---------------------------------------------------------------------------
+
+__global__ void pad_model_kernel(const float* __restrict__ vel, float* __restrict__ vpad, int nx,
+                                 int nz, int ne, int dimx, int dimz, int pitch) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    // read: consecutive threads walk z (contiguous in the user layout)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int cl = ty + 8 * j;
+        const int col = c0 + cl, row = r0 + tx;
+        const int ix = min(max(col - ne, 0), nx - 1);
+        const int iz = min(max(row - ne, 0), nz - 1);
+        tile[cl][tx] = vel[(long long)ix * nz + iz];
+    }
+    __syncthreads();
+    // write: consecutive threads walk x (contiguous in the padded layout)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int rl = ty + 8 * j;
+        const int row = r0 + rl, col = c0 + tx;
+        if (row < dimz && col < pitch)
+            vpad[(long long)row * pitch + col] = col < dimx ? tile[tx][rl] : 0.f;
+    }
+}
+
+__global__ void reduce_grad_kernel(const float* __restrict__ acc, const float* __restrict__ comp,
+                                   int nacc, long long slot_elems, int pitch, int ne, int nx,
+                                   int nz, int kahan, float* __restrict__ out) {
+    __shared__ float tile[32][33];
+    const int z0 = blockIdx.y * 32, x0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int zl = ty + 8 * j;
+        const int iz = z0 + zl, ix = x0 + tx;
+        float g = 0.f;
+        if (iz < nz && ix < nx) {
+            const long long off = (long long)(iz + ne) * pitch + (ix + ne);
+            if (kahan) {
+                float s = 0.f, cc = 0.f;
+                for (int k = 0; k < nacc; ++k) {
+                    kahan_add(s, cc, acc[k * slot_elems + off]);
+                    kahan_add(s, cc, -comp[k * slot_elems + off]);
+                }
+                g = __fsub_rn(s, cc);
+            } else {
+                g = acc[off];
+                for (int k = 1; k < nacc; ++k) g = __fadd_rn(g, acc[k * slot_elems + off]);
+            }
+        }
+        tile[zl][tx] = g;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int xl = ty + 8 * j;
+        const int ix = x0 + xl, iz = z0 + tx;
+        if (ix < nx && iz < nz) out[(long long)ix * nz + iz] = tile[tx][xl];
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
+                        const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
+                        const CUtensorMap& tm_vel, const StepArgs& a, cudaStream_t stream) {
+    switch (order) {
+        case 2: return launch_arith<2>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
+        case 4: return launch_arith<4>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
+        case 8: return launch_arith<8>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t prepare_step(int order, bool exact, LaunchShape shape) {
+    const CUtensorMap none{};
+    for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
+        cudaError_t e = cudaErrorInvalidValue;
+        switch (order) {
+            case 2: e = launch_arith<2>(exact, m, shape, none, none, none, nullptr, nullptr); break;
+            case 4: e = launch_arith<4>(exact, m, shape, none, none, none, nullptr, nullptr); break;
+            case 8: e = launch_arith<8>(exact, m, shape, none, none, none, nullptr, nullptr); break;
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_pad_model(const float* vel_user, float* vpad, int nx, int nz, int ne,
+                             int dimx, int dimz, int pitch, cudaStream_t stream) {
+    dim3 grid((pitch + 31) / 32, (dimz + 31) / 32);
+    pad_model_kernel<<<grid, dim3(32, 8), 0, stream>>>(vel_user, vpad, nx, nz, ne, dimx, dimz, pitch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reduce_grad(const float* acc, const float* acc_comp, int nacc,
+                               long long slot_elems, int pitch, int ne, int nx, int nz,
+                               int kahan, float* grad_user, cudaStream_t stream) {
+    dim3 grid((nx + 31) / 32, (nz + 31) / 32);
+    reduce_grad_kernel<<<grid, dim3(32, 8), 0, stream>>>(acc, acc_comp, nacc, slot_elems, pitch, ne,
+                                                        nx, nz, kahan, grad_user);
+    return cudaGetLastError();
+}
+
+}  // namespace twi

@@ -1,0 +1,182 @@
+"""Python owner of a C-ABI plan: one velocity model, a batch of shots and a
+device workspace allocated through PyTorch's caching allocator.
+
+The workspace holds the model, wavelet, gathers/residual and gradient
+regions (exposed here as tensor views) plus the internal wavefield slots,
+checkpoints and gradient accumulators.  All work is enqueued on the current
+PyTorch stream.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _capi
+from ._capi import Layout, Problem, check
+
+
+@dataclass
+class PlanOptions:
+    """Tuning and numerics switches of a plan.
+
+    exact:       reproduce the reference CPU propagator's arithmetic bit for
+                 bit (FP32 storage, FP64 where its C++ promotes); False uses
+                 plain FP32 with FMA.
+    accumulate:  "kahan" (compensated FP32 over time steps and shots) or
+                 "plain" (per-shot FP32 sums added in shot order, the
+                 reference's own order -> bit-identical gradients).
+    ckpt_interval: steps between saved wavefield pairs (0 = sqrt(2 nt)).
+    shots_per_cta, rows_per_warp: launch shape (0 = default).
+    use_graphs:  capture the time loops into CUDA graphs.
+    """
+
+    exact: bool = True
+    accumulate: str = "kahan"
+    ckpt_interval: int = 0
+    shots_per_cta: int = 0
+    rows_per_warp: int = 0
+    use_graphs: bool = True
+
+
+def _stream_handle() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def footprint_bytes(nx, nz, nt, nshots, order=4, wavelet_per_shot=False,
+                    options: PlanOptions | None = None) -> int:
+    """Workspace bytes a plan of this size needs (for HBM admission)."""
+    o = options or PlanOptions()
+    prob = _problem(nx, nz, nt, 10.0, 1e-3, nshots, order, wavelet_per_shot, o)
+    L = _capi.lib()
+    h = ctypes.c_void_p()
+    check(L.twi_plan_create(ctypes.byref(prob), ctypes.byref(h)))
+    lay = Layout()
+    try:
+        check(L.twi_plan_layout(h, ctypes.byref(lay)))
+    finally:
+        L.twi_plan_destroy(h)
+    return int(lay.workspace_bytes)
+
+
+def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions) -> Problem:
+    if o.accumulate not in ("kahan", "plain"):
+        raise ValueError("accumulate must be 'kahan' or 'plain'")
+    return Problem(order=int(order), nx=int(nx), nz=int(nz), nt=int(nt), h=float(h), dt=float(dt),
+                   nshots=int(nshots), ckpt_interval=int(o.ckpt_interval), exact=int(bool(o.exact)),
+                   accumulate=0 if o.accumulate == "kahan" else 1,
+                   shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
+                   use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)))
+
+
+class ShotPlan:
+    """A batch of `nshots` shots over one (nx, nz) model."""
+
+    def __init__(self, nx, nz, h, dt, nt, order=4, nshots=1, wavelet_per_shot=False,
+                 options: PlanOptions | None = None, device=None):
+        if not torch.cuda.is_available():
+            raise _capi.TwiError(_capi.TWI_ERR_CUDA, "torchwi_b200 needs a CUDA device")
+        self.options = options or PlanOptions()
+        self.nx, self.nz, self.nt, self.order = int(nx), int(nz), int(nt), int(order)
+        self.h, self.dt, self.nshots = float(h), float(dt), int(nshots)
+        self.wavelet_per_shot = bool(wavelet_per_shot)
+        self.device = torch.device(device) if device is not None else torch.device(
+            "cuda", torch.cuda.current_device())
+        self._lib = _capi.lib()
+        prob = _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, self.options)
+        self._h = ctypes.c_void_p()
+        check(self._lib.twi_plan_create(ctypes.byref(prob), ctypes.byref(self._h)))
+        self.layout = Layout()
+        check(self._lib.twi_plan_layout(self._h, ctypes.byref(self.layout)))
+        with torch.cuda.device(self.device):
+            self.workspace = torch.empty(int(self.layout.workspace_bytes), dtype=torch.uint8,
+                                         device=self.device)
+            check(self._lib.twi_plan_bind(self._h, ctypes.c_void_p(self.workspace.data_ptr()),
+                                          ctypes.c_size_t(self.workspace.numel())))
+        lay = self.layout
+        S, nt_ = self.nshots, self.nt
+        self.vel = self._view(lay.vel, (self.nx, self.nz))
+        self.wavelet = self._view(lay.wavelet, (S if self.wavelet_per_shot else 1, nt_))
+        self.gathers = self._view(lay.gathers, (S, nt_, self.nx))
+        self.resid = self._view(lay.resid, (S, nt_, self.nx))
+        self.grad = self._view(lay.grad, (self.nx, self.nz))
+        self._have_ckpt = False
+
+    def _view(self, offset, shape):
+        n = int(np.prod(shape))
+        return self.workspace[offset:offset + 4 * n].view(torch.float32).view(*shape)
+
+    # -- inputs -----------------------------------------------------------------
+    def set_shots(self, sx, sy, ry):
+        """Shot and receiver positions in metres, one entry per shot."""
+        def arr(a):
+            a = a.detach().cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a)
+            a = np.ascontiguousarray(np.broadcast_to(a.astype(np.float32).reshape(-1),
+                                                     (self.nshots,)))
+            return a
+        self._sx, self._sy, self._ry = arr(sx), arr(sy), arr(ry)
+        f = ctypes.POINTER(ctypes.c_float)
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_plan_set_shots(
+                self._h, self._sx.ctypes.data_as(f), self._sy.ctypes.data_as(f),
+                self._ry.ctypes.data_as(f), _stream_handle()))
+        self._have_ckpt = False
+
+    def set_model(self, vel: torch.Tensor):
+        """Velocity (nx, nz), z fastest (the reference's user layout)."""
+        if tuple(vel.shape) != (self.nx, self.nz):
+            raise ValueError(f"velocity must have shape {(self.nx, self.nz)}, got {tuple(vel.shape)}")
+        with torch.cuda.device(self.device):
+            self.vel.copy_(vel.detach().to(self.device, torch.float32, non_blocking=True))
+            check(self._lib.twi_plan_set_model(self._h, _stream_handle()))
+        self._have_ckpt = False
+
+    def set_wavelet(self, w):
+        w = w if isinstance(w, torch.Tensor) else torch.as_tensor(np.asarray(w))
+        w = w.detach().to(self.device, torch.float32, non_blocking=True)
+        self.wavelet.copy_(w.reshape(self.wavelet.shape) if w.numel() == self.wavelet.numel()
+                           else w.reshape(1, -1).expand_as(self.wavelet))
+
+    # -- passes -----------------------------------------------------------------
+    def forward(self, save_checkpoints=True) -> torch.Tensor:
+        """Run all shots; returns the gathers view [nshots, nt, nx]."""
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_forward(self._h, int(bool(save_checkpoints)), _stream_handle()))
+        self._have_ckpt = bool(save_checkpoints)
+        return self.gathers
+
+    def gradient(self, resid: torch.Tensor | None = None) -> torch.Tensor:
+        """Adjoint pass from `resid` [nshots, nt, nx] (already in the resid
+        region when None); returns the (nx, nz) gradient view."""
+        with torch.cuda.device(self.device):
+            if resid is not None:
+                self.resid.copy_(resid.detach().to(self.device, torch.float32).reshape(self.resid.shape))
+            check(self._lib.twi_gradient(self._h, _stream_handle()))
+        return self.grad
+
+    def profile(self, mode: int, repeats: int = 20) -> float:
+        """Mean device milliseconds per launch of one kernel mode (0 forward,
+        1 recompute, 2 adjoint) at steady state, all shots."""
+        ms = ctypes.c_float()
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_plan_profile(self._h, int(mode), int(repeats), ctypes.byref(ms),
+                                             _stream_handle()))
+        return float(ms.value)
+
+    def check(self):
+        """Synchronise and raise if a kernel set the device error word."""
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_plan_check(self._h, _stream_handle()))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                torch.cuda.synchronize(self.device)
+            except Exception:
+                pass
+            self._lib.twi_plan_destroy(h)
+            self._h = None
