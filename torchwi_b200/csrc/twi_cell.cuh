@@ -132,6 +132,20 @@ __device__ __forceinline__ float virt_of(float um, float u, float up, float v, f
     return cons / (v * v * v) * ((um - 2.0f * u) + up);
 }
 
+// The same virtual source split into a per-cell coefficient q = cons/(v*v*v)
+// (constant over time, computed once) and the per-step product; bit-identical
+// to virt_of.
+template <bool EXACT>
+__device__ __forceinline__ float virt_coef(float v, float cons) {
+    if constexpr (EXACT) return __fdiv_rn(cons, __fmul_rn(__fmul_rn(v, v), v));
+    return cons / (v * v * v);
+}
+template <bool EXACT>
+__device__ __forceinline__ float virt_from_coef(float q, float um, float u, float up) {
+    if constexpr (EXACT) return __fmul_rn(q, __fadd_rn(__fsub_rn(um, __fmul_rn(2.0f, u)), up));
+    return q * ((um - 2.0f * u) + up);
+}
+
 // Gradient term  -virt * lambda  (propagator_cpu.cpp:143-144).
 template <bool EXACT>
 __device__ __forceinline__ float grad_term(float virt, float lam) {

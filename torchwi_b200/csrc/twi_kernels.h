@@ -31,6 +31,7 @@ struct StepArgs {
     int dimx, dimz, pitch, nx, nz;
     long long slot_elems;
     float* fields;
+    const float* vel;           // padded velocity [dimz][pitch] (boundary cells)
     int prev_base, prev_stride;
     int cur_base, cur_stride;
     int next_base, next_stride;

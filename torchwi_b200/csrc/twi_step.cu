@@ -62,8 +62,37 @@ __device__ __forceinline__ float4 ld4(const float* p) {
     return *reinterpret_cast<const float4*>(p);
 }
 
+// Cells that are not plain interior cells of a lane's float4: the Keys pads,
+// the free-surface rows, columns past the grid and interior cells next to
+// them.  Kept out of line so the hot loop stays small enough for the
+// instruction cache.  U2/U1 point at the cell inside the staged u^n / u^{n-1}
+// tiles (row pitch kBoxX).
+template <int ORDER, bool EXACT>
+__device__ __noinline__ float edge_cell(const float* U2, const float* U1, float v, float dtoh2,
+                                        int r, int cc, int dimx, int dimz, float h2, float dt2,
+                                        float hdt) {
+    constexpr int NE = ORDER / 2;
+    if (r >= dimz || cc >= dimx || r < NE) return 0.f;          // outside / free surface
+    if (r >= dimz - NE)                                          // bottom pad, all columns
+        return keys_cell<EXACT>(U2[0], U2[-kBoxX], U2[-2 * kBoxX], U1[0], U1[-kBoxX], v, h2,
+                                dt2, hdt);
+    if (cc < NE)                                                 // left pad
+        return keys_cell<EXACT>(U2[0], U2[1], U2[2], U1[0], U1[1], v, h2, dt2, hdt);
+    if (cc >= dimx - NE)                                         // right pad
+        return keys_cell<EXACT>(U2[0], U2[-1], U2[-2], U1[0], U1[-1], v, h2, dt2, hdt);
+    float lf[NE], rt[NE], up[NE], dn[NE];
+#pragma unroll
+    for (int d = 1; d <= NE; ++d) {
+        lf[d - 1] = U2[-d];
+        rt[d - 1] = U2[d];
+        up[d - 1] = U2[-d * kBoxX];
+        dn[d - 1] = U2[d * kBoxX];
+    }
+    return interior_update<ORDER, EXACT>(lf, rt, up, dn, U2[0], U1[0], vv_of<EXACT>(v, dtoh2));
+}
+
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32)
+__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
             const __grid_constant__ CUtensorMap tm_vel, const StepArgs a) {
     using S = Smem<ORDER, RZ, WZ>;
@@ -111,8 +140,10 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
     const int rl0 = warp * RZ;           // first tile-local row of this warp
     const int c = x0 + 4 * lane;         // first column of this lane
     const int cs = kHaloX + 4 * lane;    // its shared-memory column
+    const bool col_ok = c < a.dimx;
+    // the lane's four columns are all interior (stencil) columns
+    const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
 
-    // -- velocity tile: kept in registers for all shots --------------------------
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
         if (__syncthreads_or(!ok)) {
@@ -120,17 +151,27 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
             return;
         }
     }
-    float4 vreg[RZ], vvreg[RZ];
+    // per-cell constants over all shots: v*v*dt^2/h^2, and for the recompute
+    // the virtual-source coefficient; v itself stays in shared memory
+    float4 vvreg[RZ];
+    float4 qreg[MODE == kModeRecompute ? RZ : 1];
 #pragma unroll
     for (int rr = 0; rr < RZ; ++rr) {
-        vreg[rr] = ld4(vs + (rl0 + rr) * kTileX + 4 * lane);
-        vvreg[rr] = make_float4(vv_of<EXACT>(vreg[rr].x, a.dtoh2), vv_of<EXACT>(vreg[rr].y, a.dtoh2),
-                                vv_of<EXACT>(vreg[rr].z, a.dtoh2), vv_of<EXACT>(vreg[rr].w, a.dtoh2));
+        const float4 v4 = ld4(vs + (rl0 + rr) * kTileX + 4 * lane);
+        vvreg[rr] = make_float4(vv_of<EXACT>(v4.x, a.dtoh2), vv_of<EXACT>(v4.y, a.dtoh2),
+                                vv_of<EXACT>(v4.z, a.dtoh2), vv_of<EXACT>(v4.w, a.dtoh2));
+        if constexpr (MODE == kModeRecompute) {
+            // padding columns hold v = 0: keep their (never stored) coefficient finite
+            const float4 w4 = col_ok ? v4 : make_float4(1.f, 1.f, 1.f, 1.f);
+            qreg[rr] = make_float4(virt_coef<EXACT>(w4.x != 0.f ? w4.x : 1.f, a.cons),
+                                   virt_coef<EXACT>(w4.y != 0.f ? w4.y : 1.f, a.cons),
+                                   virt_coef<EXACT>(w4.z != 0.f ? w4.z : 1.f, a.cons),
+                                   virt_coef<EXACT>(w4.w != 0.f ? w4.w : 1.f, a.cons));
+        }
     }
 
-    // -- Kahan accumulators of this CTA's shot group (adjoint) -----------------------
+    // Kahan accumulators of this CTA's shot group (adjoint)
     float4 gsum[MODE == kModeAdjoint ? RZ : 1], gcmp[MODE == kModeAdjoint ? RZ : 1];
-    const bool col_ok = c < a.dimx;
     if constexpr (MODE == kModeAdjoint) {
         if (a.acc_mode == kAccKahanPerGroup) {
             const long long slot = a.acc_base + blockIdx.z;
@@ -164,7 +205,8 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
         // virtual source of this step for the warp's rows (adjoint)
         float4 vin[MODE == kModeAdjoint ? RZ : 1];
         if constexpr (MODE == kModeAdjoint) {
-            const float* vbase = a.virt_in + (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems;
+            const float* vbase =
+                a.virt_in + (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems;
 #pragma unroll
             for (int rr = 0; rr < RZ; ++rr) {
                 const int r = z0 + rl0 + rr;
@@ -217,12 +259,12 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
             }
             const float4 um4 = ld4(u1s + (rl + 1) * kBoxX + cs);
             const float um[4] = {um4.x, um4.y, um4.z, um4.w};
+            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 
             const bool row_ok = r < a.dimz;
             const bool interior_row = r >= NE && r < a.dimz - NE;
-            const bool fast = interior_row && c >= NE && c + 3 < a.dimx - NE;
             float out[4];
-            if (fast) {
+            if (interior_row && cols_interior) {
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     float lf[NE], rt[NE], up[NE], dn[NE];
@@ -238,62 +280,40 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
                                                            comp(vvreg[rr], m));
                 }
             } else {
+                const float* U2 = u2s + (rl + HZ) * kBoxX + cs;
+                const float* U1 = u1s + (rl + 1) * kBoxX + cs;
 #pragma unroll
-                for (int m = 0; m < 4; ++m) {
-                    const int cc = c + m;
-                    out[m] = 0.f;
-                    if (row_ok && cc < a.dimx && r >= NE) {
-                        const float* U2 = u2s + (rl + HZ) * kBoxX + cs + m;
-                        const float* U1 = u1s + (rl + 1) * kBoxX + cs + m;
-                        const float v = comp(vreg[rr], m);
-                        if (r >= a.dimz - NE) {          // bottom pad (all columns)
-                            out[m] = keys_cell<EXACT>(U2[0], U2[-kBoxX], U2[-2 * kBoxX], U1[0],
-                                                      U1[-kBoxX], v, a.h2, a.dt2, a.hdt);
-                        } else if (cc < NE) {            // left pad
-                            out[m] = keys_cell<EXACT>(U2[0], U2[1], U2[2], U1[0], U1[1], v, a.h2,
-                                                      a.dt2, a.hdt);
-                        } else if (cc >= a.dimx - NE) {  // right pad
-                            out[m] = keys_cell<EXACT>(U2[0], U2[-1], U2[-2], U1[0], U1[-1], v,
-                                                      a.h2, a.dt2, a.hdt);
-                        } else {                          // interior
-                            float lf[NE], rt[NE], up[NE], dn[NE];
-#pragma unroll
-                            for (int d = 1; d <= NE; ++d) {
-                                lf[d - 1] = U2[-d];
-                                rt[d - 1] = U2[d];
-                                up[d - 1] = U2[-d * kBoxX];
-                                dn[d - 1] = U2[d * kBoxX];
-                            }
-                            out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, U2[0], U1[0],
-                                                                   comp(vvreg[rr], m));
-                        }
-                    }
-                }
+                for (int m = 0; m < 4; ++m)
+                    out[m] = edge_cell<ORDER, EXACT>(U2 + m, U1 + m, comp(v4, m), a.dtoh2, r, c + m,
+                                                     a.dimx, a.dimz, a.h2, a.dt2, a.hdt);
             }
 
             // sources: only cells updated by the interior stencil receive them
-            // (the reference adds before Keys, which overwrites pad cells).
+            // (the reference adds before Keys, which overwrites pad cells)
             if constexpr (MODE != kModeAdjoint) {
-                if (r == src_r && interior_row) {
+                if (r == src_r && interior_row && src_c >= c && src_c < c + 4 && src_c >= NE &&
+                    src_c < a.dimx - NE) {
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
-                        if (c + m == src_c && src_c >= NE && src_c < a.dimx - NE)
-                            out[m] = add_injection<EXACT>(out[m], wamp, comp(vreg[rr], m), a.dt2);
+                        if (c + m == src_c)
+                            out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
                 }
             } else {
                 if (r == rec_r && interior_row) {
-                    const float* rs = a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
+                    const float* rs =
+                        a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         const int cc = c + m;
                         if (cc >= NE && cc < NE + a.nx)
-                            out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(vreg[rr], m), a.dt2);
+                            out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
                     }
                 }
             }
 
             if (row_ok && col_ok) {
-                float* dst = a.fields + (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
+                float* dst = a.fields +
+                             (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
                              (long long)r * a.pitch + c;
                 *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
             }
@@ -311,15 +331,13 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 
             if constexpr (MODE == kModeRecompute) {
                 if (row_ok && col_ok) {
+                    // every grid cell, as the reference stores it (pads included)
                     float vo[4];
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const int cc = c + m;
-                        // every grid cell, as the reference stores it (pads included)
-                        vo[m] = cc < a.dimx
-                                    ? virt_of<EXACT>(um[m], c4[m], out[m], comp(vreg[rr], m), a.cons)
+                    for (int m = 0; m < 4; ++m)
+                        vo[m] = c + m < a.dimx
+                                    ? virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m])
                                     : 0.f;
-                    }
                     float* p = a.virt_out +
                                (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                (long long)r * a.virt_pitch + c;
@@ -340,8 +358,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
                     if (a.acc_mode == kAccKahanPerGroup) {
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
-                            const int cc = c + m;
-                            if (cc < a.dimx) {
+                            if (c + m < a.dimx) {
                                 float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
                                 kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
                                 set_comp(gsum[rr], m, sm);
@@ -354,12 +371,10 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
                             (long long)r * a.pitch + c);
                         float4 gv = *g;
 #pragma unroll
-                        for (int m = 0; m < 4; ++m) {
-                            const int cc = c + m;
-                            if (cc < a.dimx)
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m < a.dimx)
                                 set_comp(gv, m, __fadd_rn(comp(gv, m),
                                                           grad_term<EXACT>(comp(vin[rr], m), out[m])));
-                        }
                         *g = gv;
                     }
                 }
