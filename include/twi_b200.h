@@ -75,6 +75,26 @@ int twi_fdm_forward_only(float* frd, float* u1, float* u2, float* u3, const floa
                          const float* w, int order, int dimx, int dimy, int nt, float h,
                          float dt, float sx, float sy, float ry, void* stream);
 
+/* Forward modelling of one shot that allocates no device memory, for
+ * callers that cannot call cudaMalloc (code running inside another
+ * framework's memory pool or a fixed arena, hosts that forbid allocation
+ * after start-up, callers that must avoid an allocation's implicit
+ * synchronisation).  No counterpart in the reference.
+ *
+ * Same inputs and output as twi_fdm_forward_only, without the unused
+ * u1/u2/u3; `vel` and `frd` are device pointers, `w` host or device.  The
+ * scratch is a file-scope device array of 32 MiB reserved on every GPU that
+ * loads the library: grids need
+ *   5 * roundup(dimx,128) * dimy * 4 + nt * 4 bytes (+ < 2 KiB)
+ * to fit, larger ones are rejected with TWI_ERR_INVALID.  The first call on
+ * a device looks up the scratch address (cudaGetSymbolAddress) and should
+ * come before any stream capture.  All calls share the scratch: calls whose
+ * work overlaps on the GPU race, so issue them on one stream or synchronise
+ * between them.  Synchronises `stream` before returning. */
+int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const float* w, int order,
+                                 int dimx, int dimy, int nt, float h, float dt, float sx,
+                                 float sy, float ry, void* stream);
+
 /* ------------------------------------------------------------------------
  * 2. Plan API
  *

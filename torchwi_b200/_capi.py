@@ -59,6 +59,7 @@ SIGNATURES = {
     "twi_fdm_forward": [_vp] * 7 + [_i] * 4 + [_f] * 5 + [_vp],
     "twi_fdm_backward": [_vp] * 7 + [_i] * 4 + [_f] * 3 + [_vp],
     "twi_fdm_forward_only": [_vp] * 6 + [_i] * 4 + [_f] * 5 + [_vp],
+    "twi_fdm_forward_only_noalloc": [_vp] * 3 + [_i] * 4 + [_f] * 5 + [_vp],
     "twi_plan_create": [ctypes.POINTER(Problem), ctypes.POINTER(_vp)],
     "twi_plan_layout": [_vp, ctypes.POINTER(Layout)],
     "twi_plan_bind": [_vp, _vp, ctypes.c_size_t],

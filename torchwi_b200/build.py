@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libtwi_b200.so")
 INCLUDE = os.path.join(REPO, "include")
-SOURCES = ["twi_step.cu", "twi_plan.cu"]
+SOURCES = ["twi_step.cu", "twi_plan.cu", "twi_noalloc.cu"]
 HEADERS = ["twi_cell.cuh", "twi_kernels.h", "twi_ptx.cuh"]
 
 NVCC_FLAGS = [

@@ -41,6 +41,15 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+namespace twi {
+// Lets other translation units of the library report through twi_last_error.
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace twi
+
+namespace {
+
 #define TWI_CUDA(expr)                                                                  \
     do {                                                                                \
         cudaError_t e_ = (expr);                                                        \
