@@ -71,8 +71,10 @@ struct LaunchShape {
     int warps;           // warps per CTA, stacked along z
 };
 
-// Launches one time step.  tm_u2 / tm_u1 / tm_vel are tensor maps over the
-// field slots (boxes with halo) and the padded velocity.
+// Launches one time step.  tm_u2 is a tensor map over the field slots with a
+// (136, TZ + order) box (4-column / ne-row halo), tm_u1 the same slots with a
+// (128, TZ) box and tm_vel the padded velocity with a (128, TZ) box, where
+// TZ = 4 * rows_per_warp.
 cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
                         const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
                         const CUtensorMap& tm_vel, const StepArgs& a, cudaStream_t stream);
@@ -85,7 +87,11 @@ cudaError_t prepare_step(int order, bool exact, LaunchShape shape);
 constexpr int kTileX = 128;                    // columns per CTA (32 lanes x float4)
 constexpr int kHaloX = 4;                      // x halo, keeps TMA x origins 16-byte aligned
 constexpr int kBoxX = kTileX + 2 * kHaloX;     // 136 columns per staged row
-__host__ __device__ constexpr int zhalo(int order) { return order / 2 > 2 ? order / 2 : 2; }
+__host__ __device__ constexpr int zhalo(int order) { return order / 2; }
+// Boundary (Keys) cells are computed by dedicated CTAs, one thread per cell
+// and this many cells per thread, ahead of the interior tiles in the grid.
+constexpr int kBoundaryCellsPerThread = 4;
+constexpr int kThreads = 128;
 
 // (nx, nz) z-fastest user model -> padded [dimz][pitch] x-fastest,
 // edge-replicated by ne cells (TimeOperator.py:55-58); columns >= dimx are 0.

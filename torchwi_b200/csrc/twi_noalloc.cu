@@ -163,7 +163,7 @@ extern "C" int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const 
     const int TZ = 16, HZ = zhalo(order);
     CUtensorMap tm_u2, tm_u1, tm_vel;
     if ((s = encode(&tm_u2, fields, dimx, dimy, 4, pitch, kBoxX, TZ + 2 * HZ)) != TWI_OK) return s;
-    if ((s = encode(&tm_u1, fields, dimx, dimy, 4, pitch, kBoxX, TZ + 1)) != TWI_OK) return s;
+    if ((s = encode(&tm_u1, fields, dimx, dimy, 4, pitch, kTileX, TZ)) != TWI_OK) return s;
     if ((s = encode(&tm_vel, vpad, dimx, dimy, 0, pitch, kTileX, TZ)) != TWI_OK) return s;
     NOALLOC_CUDA(prepare_step(order, true, shape));
 
@@ -171,6 +171,7 @@ extern "C" int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const 
     a.dimx = dimx, a.dimz = dimy, a.pitch = pitch, a.nx = nx, a.nz = nz;
     a.slot_elems = (long long)pitch * dimy;
     a.fields = fields;
+    a.vel = vpad;
     a.nshots = 1, a.spc = 1;
     const float dt2 = dt * dt, h2 = h * h;
     a.dt2 = dt2, a.h2 = h2, a.dtoh2 = dt2 / h2, a.hdt = h * dt;

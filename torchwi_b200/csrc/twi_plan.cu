@@ -198,6 +198,7 @@ struct twi_plan {
         a.nz = p.nz;
         a.slot_elems = slot_elems;
         a.fields = F(off_fields);
+        a.vel = F(off_vpad);
         a.nshots = p.nshots;
         a.spc = spc;
         const float dt2 = p.dt * p.dt, h2 = p.h * p.h;
@@ -412,8 +413,8 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
     const int TZ = P->rz * 4;
     TWI_TRY(make_map(&P->tm_u2, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kBoxX,
                      TZ + 2 * HZ));
-    TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kBoxX,
-                     TZ + 1));
+    TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
+                     TZ));
     TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
     // zero slot, error word and velocity padding columns
     TWI_CUDA(cudaMemset(P->F(P->off_fields), 0, (size_t)P->slot_elems * 4));
@@ -585,7 +586,7 @@ struct RefRun {
         TWI_CUDA(prepare_step(order, true, LaunchShape{4, 4}));
         const int TZ = 16, HZ = zhalo(order);
         TWI_TRY(make_map(&tm_u2, F(off_fields), dimx, dimz, 4, pitch, kBoxX, TZ + 2 * HZ));
-        TWI_TRY(make_map(&tm_u1, F(off_fields), dimx, dimz, 4, pitch, kBoxX, TZ + 1));
+        TWI_TRY(make_map(&tm_u1, F(off_fields), dimx, dimz, 4, pitch, kTileX, TZ));
         TWI_TRY(make_map(&tm_vel, F(off_vpad), dimx, dimz, 0, pitch, kTileX, TZ));
         return TWI_OK;
     }
@@ -601,6 +602,7 @@ struct RefRun {
         a.dimx = dimx, a.dimz = dimz, a.pitch = pitch, a.nx = nx, a.nz = nz;
         a.slot_elems = slot_elems;
         a.fields = F(off_fields);
+        a.vel = F(off_vpad);
         a.nshots = 1;
         a.spc = 1;
         const float dt2 = dt * dt, h2 = h * h;

@@ -34,10 +34,9 @@ struct Smem {
     static constexpr int NE = ORDER / 2;
     static constexpr int TZ = RZ * WZ;
     static constexpr int HZ = zhalo(ORDER);
-    static constexpr int U2_ROWS = TZ + 2 * HZ;
-    static constexpr int U1_ROWS = TZ + 1;
+    static constexpr int U2_ROWS = TZ + 2 * HZ;               // u^n with halo
     static constexpr int U2_FLOATS = round32(U2_ROWS * kBoxX);
-    static constexpr int U1_FLOATS = round32(U1_ROWS * kBoxX);
+    static constexpr int U1_FLOATS = TZ * kTileX;              // u^{n-1}, no halo
     static constexpr int STAGE_FLOATS = U2_FLOATS + U1_FLOATS;
     static constexpr int V_FLOATS = TZ * kTileX;
     static constexpr int STAGES = 2;
@@ -45,7 +44,7 @@ struct Smem {
     static constexpr size_t BYTES =
         128 /*alignment slack*/ + BAR_BYTES + size_t(V_FLOATS + STAGES * STAGE_FLOATS) * 4;
     static constexpr uint32_t U2_TX = U2_ROWS * kBoxX * 4;
-    static constexpr uint32_t U1_TX = U1_ROWS * kBoxX * 4;
+    static constexpr uint32_t U1_TX = TZ * kTileX * 4;
     static constexpr uint32_t V_TX = TZ * kTileX * 4;
 };
 
@@ -62,41 +61,91 @@ __device__ __forceinline__ float4 ld4(const float* p) {
     return *reinterpret_cast<const float4*>(p);
 }
 
-// Cells that are not plain interior cells of a lane's float4: the Keys pads,
-// the free-surface rows, columns past the grid and interior cells next to
-// them.  Kept out of line so the hot loop stays small enough for the
-// instruction cache.  U2/U1 point at the cell inside the staged u^n / u^{n-1}
-// tiles (row pitch kBoxX).
-template <int ORDER, bool EXACT>
-__device__ __noinline__ float edge_cell(const float* U2, const float* U1, float v, float dtoh2,
-                                        int r, int cc, int dimx, int dimz, float h2, float dt2,
-                                        float hdt) {
+// Number of Keys boundary cells of one shot: the left and right ne columns of
+// rows [ne, dimz-ne) and all columns of the bottom ne rows
+// (td2d_cpu.cpp:116-145).
+__host__ __device__ inline int boundary_cells(int order, int dimx, int dimz) {
+    const int ne = order / 2;
+    return 2 * ne * (dimz - 2 * ne) + ne * dimx;
+}
+
+// One boundary CTA: a strided share of the Keys cells of one shot group,
+// one thread per cell, for every shot of the group.  Neighbours come
+// straight from the slots (L2); the interior CTAs never write these cells.
+template <int ORDER, bool EXACT, int MODE>
+__device__ __forceinline__ void boundary_part(const StepArgs& a, int b, int nbc) {
     constexpr int NE = ORDER / 2;
-    if (r >= dimz || cc >= dimx || r < NE) return 0.f;          // outside / free surface
-    if (r >= dimz - NE)                                          // bottom pad, all columns
-        return keys_cell<EXACT>(U2[0], U2[-kBoxX], U2[-2 * kBoxX], U1[0], U1[-kBoxX], v, h2,
-                                dt2, hdt);
-    if (cc < NE)                                                 // left pad
-        return keys_cell<EXACT>(U2[0], U2[1], U2[2], U1[0], U1[1], v, h2, dt2, hdt);
-    if (cc >= dimx - NE)                                         // right pad
-        return keys_cell<EXACT>(U2[0], U2[-1], U2[-2], U1[0], U1[-1], v, h2, dt2, hdt);
-    float lf[NE], rt[NE], up[NE], dn[NE];
-#pragma unroll
-    for (int d = 1; d <= NE; ++d) {
-        lf[d - 1] = U2[-d];
-        rt[d - 1] = U2[d];
-        up[d - 1] = U2[-d * kBoxX];
-        dn[d - 1] = U2[d * kBoxX];
+    const int grp = b / nbc, part = b - grp * nbc;
+    const int s0 = grp * a.spc, s1 = min(s0 + a.spc, a.nshots);
+    const int side_rows = a.dimz - 2 * NE;
+    const int n_side = 2 * NE * side_rows;
+    const int nb = n_side + NE * a.dimx;
+    for (int idx = part * blockDim.x + threadIdx.x; idx < nb; idx += nbc * blockDim.x) {
+        int r, c;
+        long long db;   // offset to the first cell inwards
+        if (idx < n_side) {
+            const int side = idx / (NE * side_rows);
+            const int rem = idx - side * NE * side_rows;
+            r = NE + rem / NE;
+            const int k = rem - (rem / NE) * NE;
+            c = side == 0 ? k : a.dimx - NE + k;
+            db = side == 0 ? 1 : -1;
+        } else {
+            const int j = idx - n_side;
+            r = a.dimz - NE + j / a.dimx;
+            c = j - (j / a.dimx) * a.dimx;
+            db = -(long long)a.pitch;
+        }
+        const long long cell = (long long)r * a.pitch + c;
+        const float v = a.vel[cell];
+        const float q = MODE == kModeRecompute ? virt_coef<EXACT>(v, a.cons) : 0.f;
+        for (int s = s0; s < s1; ++s) {
+            const float* U2 = a.fields + (long long)(a.cur_base + s * a.cur_stride) * a.slot_elems + cell;
+            const float* U1 = a.fields + (long long)(a.prev_base + s * a.prev_stride) * a.slot_elems + cell;
+            const float uo = U2[0], um = U1[0];
+            const float out = keys_cell<EXACT>(uo, U2[db], U2[2 * db], um, U1[db], v, a.h2, a.dt2, a.hdt);
+            a.fields[(long long)(a.next_base + s * a.next_stride) * a.slot_elems + cell] = out;
+            if constexpr (MODE != kModeAdjoint) {
+                // a receiver row inside the bottom pad records Keys values
+                if (a.frd != nullptr && r == a.rec_row[s] && c >= NE && c < NE + a.nx)
+                    a.frd[(long long)s * a.frd_stride + (long long)a.it * a.nx + (c - NE)] = out;
+            }
+            if constexpr (MODE == kModeRecompute) {
+                a.virt_out[(long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                           (long long)r * a.virt_pitch + c] = virt_from_coef<EXACT>(q, um, uo, out);
+            }
+            if constexpr (MODE == kModeAdjoint) {
+                // pad cells are cropped by every caller; the plain per-shot sums
+                // keep them anyway so the full-grid gradient equals the reference's
+                if (a.acc_mode == kAccPlainPerShot) {
+                    const float vt = a.virt_in[(long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                               (long long)r * a.virt_pitch + c];
+                    float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + cell;
+                    *g = __fadd_rn(*g, grad_term<EXACT>(vt, out));
+                }
+            }
+        }
     }
-    return interior_update<ORDER, EXACT>(lf, rt, up, dn, U2[0], U1[0], vv_of<EXACT>(v, dtoh2));
 }
 
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
-            const __grid_constant__ CUtensorMap tm_vel, const StepArgs a) {
+            const __grid_constant__ CUtensorMap tm_vel, const StepArgs a, const int nbc) {
     using S = Smem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
+
+    const int ngroups = (a.nshots + a.spc - 1) / a.spc;
+    if ((int)blockIdx.x < nbc * ngroups) {
+        boundary_part<ORDER, EXACT, MODE>(a, blockIdx.x, nbc);
+        return;
+    }
+    const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
+    const int tiles_z = (a.dimz + TZ - 1) / TZ;
+    const int m_id = blockIdx.x - nbc * ngroups;
+    const int tile_x = m_id % tiles_x;
+    const int tile_z = (m_id / tiles_x) % tiles_z;
+    const int grp = m_id / (tiles_x * tiles_z);
 
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sbase = reinterpret_cast<unsigned char*>(
@@ -105,12 +154,11 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
     float* vs = reinterpret_cast<float*>(sbase + S::BAR_BYTES);
     float* stage0 = vs + S::V_FLOATS;
 
-    const int x0 = blockIdx.x * kTileX;
-    const int z0 = blockIdx.y * TZ;
-    const int s_begin = blockIdx.z * a.spc;
+    const int x0 = tile_x * kTileX;
+    const int z0 = tile_z * TZ;
+    const int s_begin = grp * a.spc;
     const int nloc = min(a.spc, a.nshots - s_begin);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (nloc <= 0) return;
 
     if (threadIdx.x == 0) {
         prefetch_tmap(&tm_u2);
@@ -128,8 +176,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
         uint64_t* b = &bar[1 + (k % STAGES)];
         mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
         tma_load_3d(st, &tm_u2, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
-        tma_load_3d(st + S::U2_FLOATS, &tm_u1, x0 - kHaloX, z0 - 1,
-                    a.prev_base + s * a.prev_stride, b);
+        tma_load_3d(st + S::U2_FLOATS, &tm_u1, x0, z0, a.prev_base + s * a.prev_stride, b);
     };
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
@@ -139,10 +186,13 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 
     const int rl0 = warp * RZ;           // first tile-local row of this warp
     const int c = x0 + 4 * lane;         // first column of this lane
-    const int cs = kHaloX + 4 * lane;    // its shared-memory column
+    const int cs = kHaloX + 4 * lane;    // its column in the haloed u^n tile
     const bool col_ok = c < a.dimx;
     // the lane's four columns are all interior (stencil) columns
     const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
+    bool cell_in[4];                     // per-cell interior column mask
+#pragma unroll
+    for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
 
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
@@ -161,12 +211,11 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
         vvreg[rr] = make_float4(vv_of<EXACT>(v4.x, a.dtoh2), vv_of<EXACT>(v4.y, a.dtoh2),
                                 vv_of<EXACT>(v4.z, a.dtoh2), vv_of<EXACT>(v4.w, a.dtoh2));
         if constexpr (MODE == kModeRecompute) {
-            // padding columns hold v = 0: keep their (never stored) coefficient finite
-            const float4 w4 = col_ok ? v4 : make_float4(1.f, 1.f, 1.f, 1.f);
-            qreg[rr] = make_float4(virt_coef<EXACT>(w4.x != 0.f ? w4.x : 1.f, a.cons),
-                                   virt_coef<EXACT>(w4.y != 0.f ? w4.y : 1.f, a.cons),
-                                   virt_coef<EXACT>(w4.z != 0.f ? w4.z : 1.f, a.cons),
-                                   virt_coef<EXACT>(w4.w != 0.f ? w4.w : 1.f, a.cons));
+            // columns past the grid hold v = 0: keep their (never stored) coefficient finite
+            qreg[rr] = make_float4(virt_coef<EXACT>(v4.x != 0.f ? v4.x : 1.f, a.cons),
+                                   virt_coef<EXACT>(v4.y != 0.f ? v4.y : 1.f, a.cons),
+                                   virt_coef<EXACT>(v4.z != 0.f ? v4.z : 1.f, a.cons),
+                                   virt_coef<EXACT>(v4.w != 0.f ? v4.w : 1.f, a.cons));
         }
     }
 
@@ -174,7 +223,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
     float4 gsum[MODE == kModeAdjoint ? RZ : 1], gcmp[MODE == kModeAdjoint ? RZ : 1];
     if constexpr (MODE == kModeAdjoint) {
         if (a.acc_mode == kAccKahanPerGroup) {
-            const long long slot = a.acc_base + blockIdx.z;
+            const long long slot = a.acc_base + grp;
 #pragma unroll
             for (int rr = 0; rr < RZ; ++rr) {
                 const int r = z0 + rl0 + rr;
@@ -241,6 +290,8 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
         for (int rr = 0; rr < RZ; ++rr) {
             const int rl = rl0 + rr;
             const int r = z0 + rl;
+            // the bottom pad rows and everything below belong to the boundary CTAs
+            if (r >= a.dimz - NE) break;
             win[2 * NE] = ld4(u2s + (rl + HZ + NE) * kBoxX + cs);
             const float c4[4] = {win[NE].x, win[NE].y, win[NE].z, win[NE].w};
             float L[NE], Rr[NE];   // L[k]: column c-1-k, Rr[k]: column c+4+k
@@ -257,14 +308,34 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 #pragma unroll
                 for (int kk = 0; kk < NE; ++kk) Rr[kk] = u2s[(rl + HZ) * kBoxX + cs + 4 + kk];
             }
-            const float4 um4 = ld4(u1s + (rl + 1) * kBoxX + cs);
+            const float4 um4 = ld4(u1s + rl * kTileX + 4 * lane);
             const float um[4] = {um4.x, um4.y, um4.z, um4.w};
-            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+            float* dst = a.fields + (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
+                         (long long)r * a.pitch + c;
 
-            const bool row_ok = r < a.dimz;
-            const bool interior_row = r >= NE && r < a.dimz - NE;
-            float out[4];
-            if (interior_row && cols_interior) {
+            if (r < NE) {
+                // free surface: the top rows stay zero (the reference never writes them)
+                if (col_ok) *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+                if constexpr (MODE == kModeRecompute) {
+                    if (col_ok) {
+                        float vo[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
+                        float* p = a.virt_out +
+                                   (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                   (long long)r * a.virt_pitch + c;
+                        if (a.virt_vec4) {
+                            *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
+                        } else {
+#pragma unroll
+                            for (int m = 0; m < 4; ++m)
+                                if (c + m < a.dimx) p[m] = vo[m];
+                        }
+                    }
+                }
+            } else {
+                float out[4];
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     float lf[NE], rt[NE], up[NE], dn[NE];
@@ -279,86 +350,71 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
                     out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], um[m],
                                                            comp(vvreg[rr], m));
                 }
-            } else {
-                const float* U2 = u2s + (rl + HZ) * kBoxX + cs;
-                const float* U1 = u1s + (rl + 1) * kBoxX + cs;
+                // sources land on interior cells only (validated on the host)
+                if constexpr (MODE != kModeAdjoint) {
+                    if (r == src_r && src_c >= c && src_c < c + 4) {
+                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
-                for (int m = 0; m < 4; ++m)
-                    out[m] = edge_cell<ORDER, EXACT>(U2 + m, U1 + m, comp(v4, m), a.dtoh2, r, c + m,
-                                                     a.dimx, a.dimz, a.h2, a.dt2, a.hdt);
-            }
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m == src_c)
+                                out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
+                    }
+                } else {
+                    if (r == rec_r) {
+                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                        const float* rs =
+                            a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const int cc = c + m;
+                            if (cc >= NE && cc < NE + a.nx)
+                                out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
+                        }
+                    }
+                }
 
-            // sources: only cells updated by the interior stencil receive them
-            // (the reference adds before Keys, which overwrites pad cells)
-            if constexpr (MODE != kModeAdjoint) {
-                if (r == src_r && interior_row && src_c >= c && src_c < c + 4 && src_c >= NE &&
-                    src_c < a.dimx - NE) {
+                // pad columns belong to the boundary CTAs: store interior cells only
+                if (cols_interior) {
+                    *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+                } else {
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
-                        if (c + m == src_c)
-                            out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
+                        if (cell_in[m]) dst[m] = out[m];
                 }
-            } else {
-                if (r == rec_r && interior_row) {
-                    const float* rs =
-                        a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
+
+                if constexpr (MODE != kModeAdjoint) {
+                    if (a.frd != nullptr && r == rec_r) {
+                        float* g = a.frd + (long long)s * a.frd_stride + (long long)a.it * a.nx;
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const int cc = c + m;
-                        if (cc >= NE && cc < NE + a.nx)
-                            out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
+                        for (int m = 0; m < 4; ++m) {
+                            const int cc = c + m;
+                            if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                        }
                     }
                 }
-            }
 
-            if (row_ok && col_ok) {
-                float* dst = a.fields +
-                             (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
-                             (long long)r * a.pitch + c;
-                *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
-            }
-
-            if constexpr (MODE != kModeAdjoint) {
-                if (a.frd != nullptr && r == rec_r) {
-                    float* g = a.frd + (long long)s * a.frd_stride + (long long)a.it * a.nx;
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const int cc = c + m;
-                        if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
-                    }
-                }
-            }
-
-            if constexpr (MODE == kModeRecompute) {
-                if (row_ok && col_ok) {
-                    // every grid cell, as the reference stores it (pads included)
+                if constexpr (MODE == kModeRecompute) {
                     float vo[4];
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
-                        vo[m] = c + m < a.dimx
-                                    ? virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m])
-                                    : 0.f;
+                        vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
                     float* p = a.virt_out +
                                (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                (long long)r * a.virt_pitch + c;
-                    if (a.virt_vec4) {
+                    if (cols_interior && a.virt_vec4) {
                         *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
                     } else {
 #pragma unroll
                         for (int m = 0; m < 4; ++m)
-                            if (c + m < a.dimx) p[m] = vo[m];
+                            if (cell_in[m]) p[m] = vo[m];
                     }
                 }
-            }
 
-            if constexpr (MODE == kModeAdjoint) {
-                // every grid cell, as the reference accumulates it; callers
-                // crop the model region
-                if (row_ok && col_ok) {
+                if constexpr (MODE == kModeAdjoint) {
                     if (a.acc_mode == kAccKahanPerGroup) {
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
-                            if (c + m < a.dimx) {
+                            if (cell_in[m]) {
                                 float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
                                 kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
                                 set_comp(gsum[rr], m, sm);
@@ -366,16 +422,21 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
                             }
                         }
                     } else if (a.acc_mode == kAccPlainPerShot) {
-                        float4* g = reinterpret_cast<float4*>(
-                            a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                            (long long)r * a.pitch + c);
-                        float4 gv = *g;
+                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                   (long long)r * a.pitch + c;
+                        if (cols_interior) {
+                            float4 gv = ld4(g);
 #pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (c + m < a.dimx)
+                            for (int m = 0; m < 4; ++m)
                                 set_comp(gv, m, __fadd_rn(comp(gv, m),
                                                           grad_term<EXACT>(comp(vin[rr], m), out[m])));
-                        *g = gv;
+                            *reinterpret_cast<float4*>(g) = gv;
+                        } else {
+#pragma unroll
+                            for (int m = 0; m < 4; ++m)
+                                if (cell_in[m])
+                                    g[m] = __fadd_rn(g[m], grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                        }
                     }
                 }
             }
@@ -390,7 +451,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 
     if constexpr (MODE == kModeAdjoint) {
         if (a.acc_mode == kAccKahanPerGroup) {
-            const long long slot = a.acc_base + blockIdx.z;
+            const long long slot = a.acc_base + grp;
 #pragma unroll
             for (int rr = 0; rr < RZ; ++rr) {
                 const int r = z0 + rl0 + rr;
@@ -431,9 +492,13 @@ cudaError_t launch_one(const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
     if (e != cudaSuccess || a == nullptr) return e;
     auto kern = step_kernel<ORDER, EXACT, MODE, RZ, WZ>;
-    dim3 grid((a->dimx + kTileX - 1) / kTileX, (a->dimz + S::TZ - 1) / S::TZ,
-              (a->nshots + a->spc - 1) / a->spc);
-    kern<<<grid, WZ * 32, S::BYTES, stream>>>(tm_u2, tm_u1, tm_vel, *a);
+    const long long ngroups = (a->nshots + a->spc - 1) / a->spc;
+    const int nb = boundary_cells(ORDER, a->dimx, a->dimz);
+    const int nbc = (nb + kThreads * kBoundaryCellsPerThread - 1) / (kThreads * kBoundaryCellsPerThread);
+    const long long tiles = (long long)((a->dimx + kTileX - 1) / kTileX) * ((a->dimz + S::TZ - 1) / S::TZ);
+    const long long nblocks = ngroups * (nbc + tiles);
+    if (nblocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+    kern<<<dim3((unsigned)nblocks), WZ * 32, S::BYTES, stream>>>(tm_u2, tm_u1, tm_vel, *a, nbc);
     return cudaGetLastError();
 }
 
