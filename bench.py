@@ -312,8 +312,9 @@ def run_b200(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded 3-layer model, observed gathers modelled on the true model)",
-            "config": {"workload": "config2: batched checkpointed FWI gradient, 64 shots/GPU, "
-                                   "1000x300 cells, nt=4000, order 4, Keys ABC, Kahan gradient",
+            "config": {"workload": f"{args.workload}: batched checkpointed FWI gradient, "
+                                   f"{NSHOTS} shots/GPU, 1000x300 cells, nt={NT}, order 4, "
+                                   "Keys ABC, Kahan gradient",
                        "global_batch": total_shots, "parallelism": f"shots sharded over {world} GPU(s)",
                        "arith": "fast-fp32" if args.fast else "reference-exact",
                        "ckpt_interval": plan.layout.ckpt_interval,
@@ -338,6 +339,88 @@ def run_b200(args):
         dist.destroy_process_group()
 
 
+def run_config4(args):
+    """Uneven batch: 32 seeded models (200x100 .. 2000x600 cells, 8-64 shots,
+    nt 2000-6000).  Models are packed into waves whose plan footprints fit the
+    free HBM; each wave is one PlanBatch (one launch per kernel mode and time
+    step for all its models).  Timed: forward with checkpoints, residual,
+    gradient, for every wave."""
+    import torch
+
+    from torchwi_b200 import PlanBatch, PlanOptions, ShotPlan, footprint_bytes, synthetic
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    models = synthetic.config4()
+    if args.models:
+        models = models[:args.models]
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan")
+    free, _ = torch.cuda.mem_get_info(dev)
+    budget = int(free * 0.80)
+    fps = [footprint_bytes(m.nx, m.nz, m.nt, m.nshots, 4, options=opts) for m in models]
+    obs_bytes = [4 * m.nshots * m.nt * m.nx for m in models]
+    order = sorted(range(len(models)), key=lambda i: -fps[i])
+    waves, cur, used = [], [], 0
+    for i in order:
+        need = fps[i] + obs_bytes[i]
+        if cur and used + need > budget:
+            waves.append(cur)
+            cur, used = [], 0
+        cur.append(i)
+        used += need
+    if cur:
+        waves.append(cur)
+    total_ms, shots, cells = 0.0, 0, 0
+    per_wave = []
+    for w in waves:
+        plans = []
+        for i in w:
+            m = models[i]
+            p = ShotPlan(m.nx, m.nz, m.h, m.dt, m.nt, 4, nshots=m.nshots, options=opts, device=dev)
+            p.set_wavelet(torch.from_numpy(m.w))
+            p.set_shots(m.sx, m.sy, m.ry)
+            p.set_model(torch.from_numpy(m.vel).to(dev))
+            plans.append(p)
+        batch = PlanBatch(plans)
+        obs = [g.clone() for g in batch.forward(save_checkpoints=False)]
+        starts = [torch.from_numpy(models[i].vel_start).to(dev) for i in w]
+
+        def step():
+            for p, v in zip(plans, starts):
+                p.set_model(v)
+            gathers = batch.forward(save_checkpoints=True)
+            for g, o in zip(gathers, obs):
+                g.sub_(o)
+            return batch.gradient()
+
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        batch.check()
+        ms = e0.elapsed_time(e1) / args.steps
+        total_ms += ms
+        wshots = sum(models[i].nshots for i in w)
+        wcells = sum(2 * models[i].nshots * models[i].nx * models[i].nz * models[i].nt for i in w)
+        shots += wshots
+        cells += wcells
+        per_wave.append({"models": len(w), "shots": wshots, "ms": ms,
+                         "footprint_gb": sum(fps[i] for i in w) / 1e9})
+        del batch, plans, obs, starts
+        torch.cuda.empty_cache()
+    print(json.dumps({"workload": "config4 uneven batch", "metric": "shot-gradients/s",
+                      "value": shots / (total_ms / 1e3), "unit": "shot-gradients/s",
+                      "gcell_per_s": cells / (total_ms / 1e3) / 1e9, "models": len(models),
+                      "shots": shots, "ms_total": total_ms, "waves": per_wave,
+                      "arith": "fast-fp32" if args.fast else "reference-exact",
+                      "hbm_budget_gb": budget / 1e9}), flush=True)
+
+
 def main():
     global NSHOTS, NT
     ap = argparse.ArgumentParser()
@@ -354,10 +437,21 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--shots", type=int, default=NSHOTS, help="shots per GPU")
     ap.add_argument("--nt", type=int, default=NT, help="time steps")
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+                    help="config2: the 64-shot gradient (default, the contract line); "
+                         "config3: 256 shots, nt=6000, checkpoint every 50 steps; "
+                         "config4: 32 uneven models in HBM-sized waves")
+    ap.add_argument("--models", type=int, default=0, help="config4: first N models only")
     args = ap.parse_args()
-    NSHOTS, NT = args.shots, args.nt
+    if args.workload == "config3":
+        NSHOTS, NT = 256, 6000
+        args.ckpt = args.ckpt or 50
+    else:
+        NSHOTS, NT = args.shots, args.nt
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "config4":
+        run_config4(args)
     else:
         run_b200(args)
 

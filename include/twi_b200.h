@@ -167,6 +167,32 @@ int twi_plan_check(twi_plan* plan, void* stream);
 int twi_plan_profile(twi_plan* plan, int mode, int repeats, float* ms_per_launch, void* stream);
 int twi_plan_destroy(twi_plan* plan);
 
+/* ------------------------------------------------------------------------
+ * 3. Batches of plans
+ *
+ * Several bound plans -- any grid sizes, shot counts and nt, sharing order,
+ * arithmetic and rows_per_warp -- advanced together: every time step is one
+ * launch per kernel mode covering all plans that still have work (plans
+ * with fewer steps drop out).  Results equal running each plan on its own,
+ * bit for bit.  Replaces the reference's one-shot-per-process Horovod loop
+ * for many models (examples/time/inv_torch.py:128-137).  No counterpart in
+ * the reference's native code.
+ * ------------------------------------------------------------------------ */
+
+typedef struct twi_batch twi_batch;
+
+/* Host only: checks the plans and sizes the batch's device workspace (job
+ * tables and tensor maps). */
+int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** batch);
+int twi_batch_workspace_size(const twi_batch* batch, size_t* bytes);
+/* Every plan must be bound first; rebinding a plan requires rebinding the
+ * batch. */
+int twi_batch_bind(twi_batch* batch, void* workspace, size_t bytes);
+/* twi_forward / twi_gradient of every plan, interleaved step by step. */
+int twi_batch_forward(twi_batch* batch, int save_checkpoints, void* stream);
+int twi_batch_gradient(twi_batch* batch, void* stream);
+int twi_batch_destroy(twi_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

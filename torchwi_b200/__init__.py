@@ -13,7 +13,7 @@ build it with ``python -m torchwi_b200.build``.
 """
 
 from .operator import Time2d, Time2dBatch, Time2dForward  # noqa: F401
-from .plan import PlanOptions, ShotPlan, footprint_bytes  # noqa: F401
+from .plan import PlanBatch, PlanOptions, ShotPlan, footprint_bytes  # noqa: F401
 from .source import fdgaus, ricker  # noqa: F401
 from ._capi import TwiError, TwiInvalid  # noqa: F401
 

@@ -70,6 +70,12 @@ SIGNATURES = {
     "twi_plan_check": [_vp, _vp],
     "twi_plan_profile": [_vp, _i, _i, ctypes.POINTER(ctypes.c_float), _vp],
     "twi_plan_destroy": [_vp],
+    "twi_batch_create": [ctypes.POINTER(_vp), _i, ctypes.POINTER(_vp)],
+    "twi_batch_workspace_size": [_vp, ctypes.POINTER(ctypes.c_size_t)],
+    "twi_batch_bind": [_vp, _vp, ctypes.c_size_t],
+    "twi_batch_forward": [_vp, _i, _vp],
+    "twi_batch_gradient": [_vp, _vp],
+    "twi_batch_destroy": [_vp],
 }
 _RESTYPES = {"twi_last_error": ctypes.c_char_p}
 

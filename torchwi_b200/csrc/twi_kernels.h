@@ -66,6 +66,15 @@ struct StepArgs {
     int* err;                   // device error word (bit 0: TMA wait timeout)
 };
 
+// One job of a multi-plan launch (device memory, 64-byte aligned).
+struct alignas(64) MultiJob {
+    StepArgs a;
+    int cta_begin;   // first CTA of this job in the launch
+    int plan;        // index of the plan's tensor maps (3 per plan)
+    int nbc;         // boundary CTAs per shot group
+    int ncta;        // CTAs of this job
+};
+
 struct LaunchShape {
     int rows_per_warp;   // 4 or 8
     int warps;           // warps per CTA, stacked along z
@@ -78,6 +87,14 @@ struct LaunchShape {
 cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
                         const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
                         const CUtensorMap& tm_vel, const StepArgs& a, cudaStream_t stream);
+
+// CTAs a single-plan launch of `a` uses, and its boundary CTAs per shot group.
+int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc);
+
+// One launch covering several jobs (tensor maps in device memory).
+cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
+                              const MultiJob* jobs, int njobs, long long nctas,
+                              const CUtensorMap* tmaps, cudaStream_t stream);
 
 // Set kernel attributes for all modes of (order, exact, shape) on the current
 // device.  Must run before a stream capture that launches them.

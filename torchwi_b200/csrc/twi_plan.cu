@@ -228,7 +228,13 @@ struct twi_plan {
         return TWI_OK;
     }
 
-    int enqueue_forward(bool save, cudaStream_t st) const {
+    struct Step {
+        StepMode mode;
+        StepArgs a;
+    };
+
+    // The forward pass as a list of time steps.
+    void forward_steps(bool save, std::vector<Step>& out) const {
         StepArgs a = base_args();
         a.frd = F(off_frd);
         for (int it = 0; it < p.nt; ++it) {
@@ -238,16 +244,13 @@ struct twi_plan {
             a.prev_base = pv.base, a.prev_stride = pv.stride;
             a.cur_base = cu.base, a.cur_stride = cu.stride;
             a.next_base = nx_.base, a.next_stride = nx_.stride;
-            TWI_TRY(launch(kModeForward, a, st));
+            out.push_back({kModeForward, a});
         }
-        return TWI_OK;
     }
 
-    int enqueue_gradient(cudaStream_t st) const {
-        const size_t acc_bytes = (size_t)nacc * slot_elems * 4;
-        if (cudaMemsetAsync(F(off_acc), 0, acc_bytes, st) != cudaSuccess ||
-            (kahan && cudaMemsetAsync(F(off_comp), 0, acc_bytes, st) != cudaSuccess))
-            return fail(TWI_ERR_CUDA, "memset of gradient accumulators failed");
+    // The gradient pass (without the accumulator reset and the final
+    // reduction) as a list of time steps: per segment, recompute then adjoint.
+    void gradient_steps(std::vector<Step>& out) const {
         StepArgs a = base_args();
         a.virt_out = F(off_virt);
         a.virt_in = F(off_virt);
@@ -268,7 +271,7 @@ struct twi_plan {
                 a.next_base = nx_.base, a.next_stride = nx_.stride;
                 a.virt_base = it - c0;
                 a.frd = nullptr;
-                TWI_TRY(launch(kModeRecompute, a, st));
+                out.push_back({kModeRecompute, a});
             }
             for (int it = c0 + L - 1; it >= c0; --it) {  // adjoint, reading virt
                 const long long m = (long long)p.nt - 1 - it;
@@ -278,14 +281,40 @@ struct twi_plan {
                 a.cur_base = cu.base, a.cur_stride = cu.stride;
                 a.next_base = nx_.base, a.next_stride = nx_.stride;
                 a.virt_base = it - c0;
-                TWI_TRY(launch(kModeAdjoint, a, st));
+                out.push_back({kModeAdjoint, a});
             }
         }
+    }
+
+    int gradient_prologue(cudaStream_t st) const {
+        const size_t acc_bytes = (size_t)nacc * slot_elems * 4;
+        if (cudaMemsetAsync(F(off_acc), 0, acc_bytes, st) != cudaSuccess ||
+            (kahan && cudaMemsetAsync(F(off_comp), 0, acc_bytes, st) != cudaSuccess))
+            return fail(TWI_ERR_CUDA, "memset of gradient accumulators failed");
+        return TWI_OK;
+    }
+
+    int gradient_epilogue(cudaStream_t st) const {
         cudaError_t e = launch_reduce_grad(F(off_acc), kahan ? F(off_comp) : nullptr, (int)nacc,
                                            slot_elems, pitch, ne, p.nx, p.nz, kahan ? 1 : 0,
                                            F(off_grad), st);
         if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("reduce: ") + cudaGetErrorString(e));
         return TWI_OK;
+    }
+
+    int enqueue_forward(bool save, cudaStream_t st) const {
+        std::vector<Step> steps;
+        forward_steps(save, steps);
+        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st));
+        return TWI_OK;
+    }
+
+    int enqueue_gradient(cudaStream_t st) const {
+        TWI_TRY(gradient_prologue(st));
+        std::vector<Step> steps;
+        gradient_steps(steps);
+        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st));
+        return gradient_epilogue(st);
     }
 
     void drop_graphs() {
@@ -535,6 +564,217 @@ int twi_plan_destroy(twi_plan* P) {
     P->drop_graphs();
     if (P->capture_stream) cudaStreamDestroy(P->capture_stream);
     delete P;
+    return TWI_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batches of plans: one launch per kernel mode and time step for all plans
+// ---------------------------------------------------------------------------
+
+struct twi_batch {
+    std::vector<twi_plan*> plans;
+    int order = 4;
+    bool exact = true, use_graphs = true;
+    LaunchShape shape{4, 4};
+    struct Launch {
+        StepMode mode;
+        size_t job0;   // first job in the phase's table
+        int njobs;
+        long long nctas;
+    };
+    // phases: 0 forward without checkpoints, 1 forward with, 2 gradient
+    std::vector<Launch> launches[3];
+    size_t njobs[3] = {0, 0, 0};
+    size_t off_tmaps = 0, off_jobs[3] = {0, 0, 0}, total = 0;
+    char* ws = nullptr;
+    bool built[3] = {false, false, false};
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graphs[3] = {nullptr, nullptr, nullptr};
+
+    void drop_graphs() {
+        for (auto& g : graphs)
+            if (g) cudaGraphExecDestroy(g), g = nullptr;
+    }
+
+    // Step lists of every plan for one phase.
+    void steps_of(int phase, std::vector<std::vector<twi_plan::Step>>& per) const {
+        per.assign(plans.size(), {});
+        for (size_t i = 0; i < plans.size(); ++i) {
+            if (phase == 2) plans[i]->gradient_steps(per[i]);
+            else plans[i]->forward_steps(phase == 1, per[i]);
+        }
+    }
+
+    static size_t max_steps(const std::vector<std::vector<twi_plan::Step>>& per) {
+        size_t m = 0;
+        for (const auto& v : per) m = std::max(m, v.size());
+        return m;
+    }
+
+    // Group the plans' steps tick by tick, one launch per (tick, mode), and
+    // upload the job table of the phase.
+    int build(int phase) {
+        std::vector<std::vector<twi_plan::Step>> per;
+        steps_of(phase, per);
+        std::vector<MultiJob> jobs;
+        jobs.reserve(njobs[phase]);
+        launches[phase].clear();
+        const size_t T = max_steps(per);
+        for (size_t t = 0; t < T; ++t) {
+            for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
+                Launch L{m, jobs.size(), 0, 0};
+                for (size_t i = 0; i < plans.size(); ++i) {
+                    if (t >= per[i].size() || per[i][t].mode != m) continue;
+                    MultiJob J{};
+                    J.a = per[i][t].a;
+                    J.plan = (int)i;
+                    J.ncta = step_ctas(order, shape, J.a, &J.nbc);
+                    if (J.ncta <= 0) return fail(TWI_ERR_INVALID, "batch launch too large");
+                    J.cta_begin = (int)L.nctas;
+                    L.nctas += J.ncta;
+                    ++L.njobs;
+                    jobs.push_back(J);
+                }
+                if (L.njobs) launches[phase].push_back(L);
+            }
+        }
+        if (jobs.size() != njobs[phase]) return fail(TWI_ERR_STATE, "batch job count mismatch");
+        TWI_CUDA(cudaMemcpy(ws + off_jobs[phase], jobs.data(), jobs.size() * sizeof(MultiJob),
+                            cudaMemcpyHostToDevice));
+        built[phase] = true;
+        return TWI_OK;
+    }
+
+    int enqueue(int phase, cudaStream_t st) const {
+        if (phase == 2)
+            for (twi_plan* P : plans) TWI_TRY(P->gradient_prologue(st));
+        const MultiJob* base = reinterpret_cast<const MultiJob*>(ws + off_jobs[phase]);
+        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
+        for (const Launch& L : launches[phase]) {
+            cudaError_t e = launch_step_multi(order, exact, L.mode, shape, base + L.job0, L.njobs,
+                                              L.nctas, tm, st);
+            if (e != cudaSuccess)
+                return fail(TWI_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+        }
+        if (phase == 2)
+            for (twi_plan* P : plans) TWI_TRY(P->gradient_epilogue(st));
+        return TWI_OK;
+    }
+
+    int run(int phase, cudaStream_t st) {
+        if (!built[phase]) TWI_TRY(build(phase));
+        if (!use_graphs) return enqueue(phase, st);
+        if (!graphs[phase]) {
+            if (!capture_stream)
+                TWI_CUDA(cudaStreamCreateWithFlags(&capture_stream, cudaStreamNonBlocking));
+            TWI_CUDA(cudaStreamBeginCapture(capture_stream, cudaStreamCaptureModeThreadLocal));
+            int s = enqueue(phase, capture_stream);
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(capture_stream, &g);
+            if (s != TWI_OK) {
+                if (g) cudaGraphDestroy(g);
+                return s;
+            }
+            if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&graphs[phase], g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+        }
+        TWI_CUDA(cudaGraphLaunch(graphs[phase], st));
+        return TWI_OK;
+    }
+};
+
+extern "C" {
+
+int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
+    if (!plans || !out || nplans < 1) return fail(TWI_ERR_INVALID, "need at least one plan");
+    twi_batch* B = new twi_batch();
+    for (int i = 0; i < nplans; ++i) {
+        twi_plan* P = plans[i];
+        if (!P) {
+            delete B;
+            return fail(TWI_ERR_INVALID, "null plan");
+        }
+        if (i == 0) {
+            B->order = P->p.order;
+            B->exact = P->p.exact != 0;
+            B->use_graphs = P->p.use_graphs != 0;
+            B->shape = default_shape(P->rz);
+        } else if (P->p.order != B->order || (P->p.exact != 0) != B->exact ||
+                   default_shape(P->rz).rows_per_warp != B->shape.rows_per_warp) {
+            delete B;
+            return fail(TWI_ERR_INVALID, "plans of a batch must share order, arithmetic and rows_per_warp");
+        }
+        B->plans.push_back(P);
+    }
+    for (twi_plan* P : B->plans) {
+        B->njobs[0] += P->p.nt;
+        B->njobs[1] += P->p.nt;
+        B->njobs[2] += 2 * (size_t)P->p.nt;
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
+    B->off_tmaps = take(B->plans.size() * 3 * sizeof(CUtensorMap));
+    for (int ph = 0; ph < 3; ++ph) B->off_jobs[ph] = take(B->njobs[ph] * sizeof(MultiJob));
+    B->total = off;
+    *out = B;
+    return TWI_OK;
+}
+
+int twi_batch_workspace_size(const twi_batch* B, size_t* bytes) {
+    if (!B || !bytes) return fail(TWI_ERR_INVALID, "null argument");
+    *bytes = B->total;
+    return TWI_OK;
+}
+
+int twi_batch_bind(twi_batch* B, void* workspace, size_t bytes) {
+    if (!B || !workspace) return fail(TWI_ERR_INVALID, "null argument");
+    if (bytes < B->total) return fail(TWI_ERR_NOMEM, "batch workspace too small: need " + std::to_string(B->total));
+    if (reinterpret_cast<uintptr_t>(workspace) % 256)
+        return fail(TWI_ERR_INVALID, "workspace must be 256-byte aligned");
+    for (twi_plan* P : B->plans)
+        if (!P->ws) return fail(TWI_ERR_STATE, "bind every plan before its batch");
+    B->drop_graphs();
+    B->ws = static_cast<char*>(workspace);
+    std::vector<CUtensorMap> tm;
+    for (twi_plan* P : B->plans) {
+        tm.push_back(P->tm_u2);
+        tm.push_back(P->tm_u1);
+        tm.push_back(P->tm_vel);
+    }
+    TWI_CUDA(cudaMemcpy(B->ws + B->off_tmaps, tm.data(), tm.size() * sizeof(CUtensorMap),
+                        cudaMemcpyHostToDevice));
+    for (bool& b : B->built) b = false;
+    return TWI_OK;
+}
+
+int twi_batch_forward(twi_batch* B, int save_checkpoints, void* stream) {
+    if (!B || !B->ws) return fail(TWI_ERR_STATE, "batch has no workspace");
+    for (twi_plan* P : B->plans)
+        if (!P->have_shots || !P->have_model)
+            return fail(TWI_ERR_STATE, "set shots and model of every plan before twi_batch_forward");
+    const int phase = save_checkpoints ? 1 : 0;
+    TWI_TRY(B->run(phase, static_cast<cudaStream_t>(stream)));
+    for (twi_plan* P : B->plans) P->have_ckpt = save_checkpoints != 0;
+    return TWI_OK;
+}
+
+int twi_batch_gradient(twi_batch* B, void* stream) {
+    if (!B || !B->ws) return fail(TWI_ERR_STATE, "batch has no workspace");
+    for (twi_plan* P : B->plans)
+        if (!P->have_ckpt)
+            return fail(TWI_ERR_STATE, "twi_batch_gradient needs a preceding twi_batch_forward(save_checkpoints=1)");
+    return B->run(2, static_cast<cudaStream_t>(stream));
+}
+
+int twi_batch_destroy(twi_batch* B) {
+    if (!B) return TWI_OK;
+    B->drop_graphs();
+    if (B->capture_stream) cudaStreamDestroy(B->capture_stream);
+    delete B;
     return TWI_OK;
 }
 

@@ -128,21 +128,25 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, int b, int nbc)
     }
 }
 
+// One CTA of one job (a time step of one plan): `cta` indexes the job's CTAs,
+// boundary CTAs first, then the interior tiles.  tm_u2 / tm_u1 / tm_vel may
+// live in parameter space (single-plan kernel) or global memory (multi-plan
+// kernel).
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
-step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
-            const __grid_constant__ CUtensorMap tm_vel, const StepArgs a, const int nbc) {
+__device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUtensorMap* tm_u1p,
+                                          const CUtensorMap* tm_velp, const StepArgs& a,
+                                          const int nbc, const int cta) {
     using S = Smem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
 
     const int ngroups = (a.nshots + a.spc - 1) / a.spc;
-    if ((int)blockIdx.x < nbc * ngroups) {
-        boundary_part<ORDER, EXACT, MODE>(a, blockIdx.x, nbc);
+    if (cta < nbc * ngroups) {
+        boundary_part<ORDER, EXACT, MODE>(a, cta, nbc);
         return;
     }
     const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
     const int tiles_z = (a.dimz + TZ - 1) / TZ;
-    const int m_id = blockIdx.x - nbc * ngroups;
+    const int m_id = cta - nbc * ngroups;
     const int tile_x = m_id % tiles_x;
     const int tile_z = (m_id / tiles_x) % tiles_z;
     const int grp = m_id / (tiles_x * tiles_z);
@@ -161,9 +165,9 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        prefetch_tmap(&tm_u2);
-        prefetch_tmap(&tm_u1);
-        prefetch_tmap(&tm_vel);
+        prefetch_tmap(tm_u2p);
+        prefetch_tmap(tm_u1p);
+        prefetch_tmap(tm_velp);
 #pragma unroll
         for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
         fence_barrier_init();
@@ -175,12 +179,12 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
         mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
-        tma_load_3d(st, &tm_u2, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
-        tma_load_3d(st + S::U2_FLOATS, &tm_u1, x0, z0, a.prev_base + s * a.prev_stride, b);
+        tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
+        tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, a.prev_base + s * a.prev_stride, b);
     };
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
-        tma_load_2d(vs, &tm_vel, x0, z0, &bar[0]);
+        tma_load_2d(vs, tm_velp, x0, z0, &bar[0]);
         for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
     }
 
@@ -465,12 +469,66 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
     }
 }
 
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
+            const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ StepArgs a,
+            const int nbc) {
+    step_body<ORDER, EXACT, MODE, RZ, WZ>(&tm_u2, &tm_u1, &tm_vel, a, nbc, blockIdx.x);
+}
+
+// Several plans (different grids, shots, time indices) in one launch: CTA
+// ranges of the jobs are contiguous and ascending in jobs[].cta_begin; the
+// tensor maps of plan p are tmaps[3p .. 3p+2].
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
+                  const CUtensorMap* __restrict__ tmaps) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {   // last job with cta_begin <= blockIdx.x
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].cta_begin <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const MultiJob& J = jobs[lo];
+    const CUtensorMap* tm = tmaps + 3 * J.plan;
+    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, J.nbc, blockIdx.x - J.cta_begin);
+}
+
 // ---------------------------------------------------------------------------
 // launch dispatch
 // ---------------------------------------------------------------------------
 
-// Set the dynamic shared-memory limit of one instantiation on the current
-// device (once per device; done before any stream capture).
+// A launch request: one plan (tensor maps + args in parameter space) or
+// several (job table + tensor maps in device memory); configure_only sets
+// the kernels' attributes and launches nothing.
+struct LaunchReq {
+    const CUtensorMap* t2 = nullptr;
+    const CUtensorMap* t1 = nullptr;
+    const CUtensorMap* tv = nullptr;
+    const StepArgs* a = nullptr;
+    const MultiJob* jobs = nullptr;
+    int njobs = 0;
+    long long nctas = 0;
+    const CUtensorMap* tmaps = nullptr;
+    bool multi = false;
+    bool configure_only = false;
+};
+
+template <int ORDER, int RZ, int WZ>
+int ctas_of(const StepArgs& a, int* nbc_out) {
+    using S = Smem<ORDER, RZ, WZ>;
+    const long long ngroups = (a.nshots + a.spc - 1) / a.spc;
+    const int nb = boundary_cells(ORDER, a.dimx, a.dimz);
+    const int nbc = (nb + kThreads * kBoundaryCellsPerThread - 1) / (kThreads * kBoundaryCellsPerThread);
+    const long long tiles = (long long)((a.dimx + kTileX - 1) / kTileX) * ((a.dimz + S::TZ - 1) / S::TZ);
+    if (nbc_out) *nbc_out = nbc;
+    const long long n = ngroups * (nbc + tiles);
+    return n > 0x7fffffffLL ? -1 : (int)n;
+}
+
+// Set the dynamic shared-memory limit of both kernels of one instantiation on
+// the current device (once per device; done before any stream capture).
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 cudaError_t configure_one() {
     using S = Smem<ORDER, RZ, WZ>;
@@ -481,53 +539,64 @@ cudaError_t configure_one() {
     if (dev >= 64 || (configured & (1ull << dev))) return cudaSuccess;
     e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     if (e == cudaSuccess) configured |= 1ull << dev;
     return e;
 }
 
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-cudaError_t launch_one(const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
-                       const CUtensorMap& tm_vel, const StepArgs* a, cudaStream_t stream) {
+cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     using S = Smem<ORDER, RZ, WZ>;
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
-    if (e != cudaSuccess || a == nullptr) return e;
-    auto kern = step_kernel<ORDER, EXACT, MODE, RZ, WZ>;
-    const long long ngroups = (a->nshots + a->spc - 1) / a->spc;
-    const int nb = boundary_cells(ORDER, a->dimx, a->dimz);
-    const int nbc = (nb + kThreads * kBoundaryCellsPerThread - 1) / (kThreads * kBoundaryCellsPerThread);
-    const long long tiles = (long long)((a->dimx + kTileX - 1) / kTileX) * ((a->dimz + S::TZ - 1) / S::TZ);
-    const long long nblocks = ngroups * (nbc + tiles);
-    if (nblocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-    kern<<<dim3((unsigned)nblocks), WZ * 32, S::BYTES, stream>>>(tm_u2, tm_u1, tm_vel, *a, nbc);
+    if (e != cudaSuccess || q.configure_only) return e;
+    if (q.multi) {
+        if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>
+            <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.njobs, q.tmaps);
+    } else {
+        int nbc = 0;
+        const int n = ctas_of<ORDER, RZ, WZ>(*q.a, &nbc);
+        if (n <= 0) return cudaErrorInvalidConfiguration;
+        step_kernel<ORDER, EXACT, MODE, RZ, WZ>
+            <<<dim3((unsigned)n), WZ * 32, S::BYTES, stream>>>(*q.t2, *q.t1, *q.tv, *q.a, nbc);
+    }
     return cudaGetLastError();
 }
 
 template <int ORDER, bool EXACT, int MODE>
-cudaError_t launch_shape(LaunchShape sh, const CUtensorMap& t2, const CUtensorMap& t1,
-                         const CUtensorMap& tv, const StepArgs* a, cudaStream_t st) {
-    if (sh.warps == 4 && sh.rows_per_warp == 4) return launch_one<ORDER, EXACT, MODE, 4, 4>(t2, t1, tv, a, st);
-    if (sh.warps == 4 && sh.rows_per_warp == 8) return launch_one<ORDER, EXACT, MODE, 8, 4>(t2, t1, tv, a, st);
+cudaError_t launch_shape(LaunchShape sh, const LaunchReq& q, cudaStream_t st) {
+    if (sh.warps == 4 && sh.rows_per_warp == 4) return launch_one<ORDER, EXACT, MODE, 4, 4>(q, st);
+    if (sh.warps == 4 && sh.rows_per_warp == 8) return launch_one<ORDER, EXACT, MODE, 8, 4>(q, st);
     return cudaErrorInvalidValue;
 }
 
 template <int ORDER, bool EXACT>
-cudaError_t launch_mode(StepMode mode, LaunchShape sh, const CUtensorMap& t2,
-                        const CUtensorMap& t1, const CUtensorMap& tv, const StepArgs* a,
-                        cudaStream_t st) {
+cudaError_t launch_mode(StepMode mode, LaunchShape sh, const LaunchReq& q, cudaStream_t st) {
     switch (mode) {
-        case kModeForward: return launch_shape<ORDER, EXACT, kModeForward>(sh, t2, t1, tv, a, st);
-        case kModeRecompute: return launch_shape<ORDER, EXACT, kModeRecompute>(sh, t2, t1, tv, a, st);
-        case kModeAdjoint: return launch_shape<ORDER, EXACT, kModeAdjoint>(sh, t2, t1, tv, a, st);
+        case kModeForward: return launch_shape<ORDER, EXACT, kModeForward>(sh, q, st);
+        case kModeRecompute: return launch_shape<ORDER, EXACT, kModeRecompute>(sh, q, st);
+        case kModeAdjoint: return launch_shape<ORDER, EXACT, kModeAdjoint>(sh, q, st);
     }
     return cudaErrorInvalidValue;
 }
 
 template <int ORDER>
-cudaError_t launch_arith(bool exact, StepMode mode, LaunchShape sh, const CUtensorMap& t2,
-                         const CUtensorMap& t1, const CUtensorMap& tv, const StepArgs* a,
+cudaError_t launch_arith(bool exact, StepMode mode, LaunchShape sh, const LaunchReq& q,
                          cudaStream_t st) {
-    return exact ? launch_mode<ORDER, true>(mode, sh, t2, t1, tv, a, st)
-                 : launch_mode<ORDER, false>(mode, sh, t2, t1, tv, a, st);
+    return exact ? launch_mode<ORDER, true>(mode, sh, q, st)
+                 : launch_mode<ORDER, false>(mode, sh, q, st);
+}
+
+cudaError_t launch_req(int order, bool exact, StepMode mode, LaunchShape shape, const LaunchReq& q,
+                       cudaStream_t st) {
+    switch (order) {
+        case 2: return launch_arith<2>(exact, mode, shape, q, st);
+        case 4: return launch_arith<4>(exact, mode, shape, q, st);
+        case 8: return launch_arith<8>(exact, mode, shape, q, st);
+    }
+    return cudaErrorInvalidValue;
 }
 
 // ---------------------------------------------------------------------------
@@ -600,23 +669,34 @@ __global__ void reduce_grad_kernel(const float* __restrict__ acc, const float* _
 cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
                         const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
                         const CUtensorMap& tm_vel, const StepArgs& a, cudaStream_t stream) {
+    LaunchReq q;
+    q.t2 = &tm_u2, q.t1 = &tm_u1, q.tv = &tm_vel, q.a = &a;
+    return launch_req(order, exact, mode, shape, q, stream);
+}
+
+cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
+                              const MultiJob* jobs, int njobs, long long nctas,
+                              const CUtensorMap* tmaps, cudaStream_t stream) {
+    LaunchReq q;
+    q.multi = true, q.jobs = jobs, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    return launch_req(order, exact, mode, shape, q, stream);
+}
+
+int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
+    const bool r8 = shape.rows_per_warp == 8;
     switch (order) {
-        case 2: return launch_arith<2>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
-        case 4: return launch_arith<4>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
-        case 8: return launch_arith<8>(exact, mode, shape, tm_u2, tm_u1, tm_vel, &a, stream);
+        case 2: return r8 ? ctas_of<2, 8, 4>(a, nbc) : ctas_of<2, 4, 4>(a, nbc);
+        case 4: return r8 ? ctas_of<4, 8, 4>(a, nbc) : ctas_of<4, 4, 4>(a, nbc);
+        case 8: return r8 ? ctas_of<8, 8, 4>(a, nbc) : ctas_of<8, 4, 4>(a, nbc);
     }
-    return cudaErrorInvalidValue;
+    return -1;
 }
 
 cudaError_t prepare_step(int order, bool exact, LaunchShape shape) {
-    const CUtensorMap none{};
+    LaunchReq q;
+    q.configure_only = true;
     for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
-        cudaError_t e = cudaErrorInvalidValue;
-        switch (order) {
-            case 2: e = launch_arith<2>(exact, m, shape, none, none, none, nullptr, nullptr); break;
-            case 4: e = launch_arith<4>(exact, m, shape, none, none, none, nullptr, nullptr); break;
-            case 8: e = launch_arith<8>(exact, m, shape, none, none, none, nullptr, nullptr); break;
-        }
+        cudaError_t e = launch_req(order, exact, m, shape, q, nullptr);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -180,3 +180,53 @@ class ShotPlan:
                 pass
             self._lib.twi_plan_destroy(h)
             self._h = None
+
+
+class PlanBatch:
+    """Several ShotPlans (any grid sizes, shot counts and nt; same order,
+    arithmetic and rows_per_warp) advanced together: each time step is one
+    launch per kernel mode covering every plan.  Results equal running each
+    plan on its own, bit for bit.  Set each plan's wavelet, shots and model
+    as usual; outputs land in each plan's own regions (gathers, grad)."""
+
+    def __init__(self, plans: list[ShotPlan]):
+        if not plans:
+            raise ValueError("PlanBatch needs at least one plan")
+        self.plans = list(plans)
+        self.device = plans[0].device
+        self._lib = _capi.lib()
+        arr = (ctypes.c_void_p * len(plans))(*[p._h for p in plans])
+        self._h = ctypes.c_void_p()
+        check(self._lib.twi_batch_create(arr, len(plans), ctypes.byref(self._h)))
+        n = ctypes.c_size_t()
+        check(self._lib.twi_batch_workspace_size(self._h, ctypes.byref(n)))
+        with torch.cuda.device(self.device):
+            self.workspace = torch.empty(max(int(n.value), 256), dtype=torch.uint8, device=self.device)
+            check(self._lib.twi_batch_bind(self._h, ctypes.c_void_p(self.workspace.data_ptr()),
+                                           ctypes.c_size_t(self.workspace.numel())))
+
+    def forward(self, save_checkpoints=True):
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_batch_forward(self._h, int(bool(save_checkpoints)), _stream_handle()))
+        for p in self.plans:
+            p._have_ckpt = bool(save_checkpoints)
+        return [p.gathers for p in self.plans]
+
+    def gradient(self):
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_batch_gradient(self._h, _stream_handle()))
+        return [p.grad for p in self.plans]
+
+    def check(self):
+        for p in self.plans:
+            p.check()
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                torch.cuda.synchronize(self.device)
+            except Exception:
+                pass
+            self._lib.twi_batch_destroy(h)
+            self._h = None
