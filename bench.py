@@ -421,6 +421,56 @@ def run_config4(args):
                       "hbm_budget_gb": budget / 1e9}), flush=True)
 
 
+def run_serve(args):
+    """Serving stream (config 5): Poisson arrivals of forward and gradient
+    requests on a resident pool of four grid sizes, replayed in real time
+    through the continuous-batching server; the same trace through the plain
+    per-request form (each request alone, FIFO) gives the comparison.
+    Observed gathers are zero (the residual is the modelled data): the work is
+    identical to real data.  The sample size is bounded by --requests,
+    --max-shots and --nt-max so one rate point takes about a minute."""
+    import torch
+
+    from torchwi_b200 import PlanOptions, synthetic
+    from torchwi_b200.serve import Request, Server, fifo_latencies, plain_service_times, run_stream
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan")
+    out = []
+    for rate in args.rates:
+        models_np, reqs_np = synthetic.config5(rate, nreq=args.requests, max_shots=args.max_shots,
+                                               nt_range=(args.nt_min, args.nt_max))
+        models = {k: torch.from_numpy(v).to(dev) for k, v in models_np.items()}
+        mk = lambda: [Request(**r) for r in reqs_np]
+        # warm the kernels once with the first request
+        srv = Server(models, h=10.0, dt=1e-3, options=opts, max_requests=64, device=dev)
+        warm = mk()[:1]
+        srv.submit(warm[0])
+        while srv.busy():
+            srv.poll(64)
+        srv = Server(models, h=10.0, dt=1e-3, options=opts, max_requests=64, device=dev)
+        reqs = mk()
+        stats = run_stream(srv, reqs, ticks=args.ticks)
+        svc = plain_service_times(models, mk(), 10.0, 1e-3, options=opts, device=dev)
+        lat = fifo_latencies([r["arrival"] for r in reqs_np], svc)
+        shots = sum(len(r["sx"]) for r in reqs_np)
+        makespan = float(np.max(lat + np.array([r["arrival"] for r in reqs_np])))
+        out.append({"rate_req_s": rate, **stats,
+                    "shots_per_s": shots / stats["seconds"],
+                    "plain": {"throughput_req_s": len(reqs) / makespan,
+                              "p50_s": float(np.percentile(lat, 50)),
+                              "p99_s": float(np.percentile(lat, 99)),
+                              "service_s_total": float(sum(svc))}})
+        del srv
+        torch.cuda.empty_cache()
+    print(json.dumps({"workload": "config5 serving stream", "requests_per_rate": args.requests,
+                      "max_shots": args.max_shots, "nt_range": [args.nt_min, args.nt_max],
+                      "grids": [list(g) for g in synthetic.SERVE_GRIDS],
+                      "arith": "fast-fp32" if args.fast else "reference-exact",
+                      "points": out}), flush=True)
+
+
 def main():
     global NSHOTS, NT
     ap = argparse.ArgumentParser()
@@ -437,7 +487,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--shots", type=int, default=NSHOTS, help="shots per GPU")
     ap.add_argument("--nt", type=int, default=NT, help="time steps")
-    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4"],
+    ap.add_argument("--rates", type=float, nargs="+", default=[5.0, 200.0])
+    ap.add_argument("--requests", type=int, default=16)
+    ap.add_argument("--max-shots", type=int, default=32)
+    ap.add_argument("--nt-min", type=int, default=2000)
+    ap.add_argument("--nt-max", type=int, default=4000)
+    ap.add_argument("--ticks", type=int, default=64)
+    ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "serve"],
                     help="config2: the 64-shot gradient (default, the contract line); "
                          "config3: 256 shots, nt=6000, checkpoint every 50 steps; "
                          "config4: 32 uneven models in HBM-sized waves")
@@ -452,6 +508,8 @@ def main():
         run_reference(args)
     elif args.workload == "config4":
         run_config4(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_b200(args)
 

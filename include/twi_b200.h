@@ -120,6 +120,8 @@ typedef struct twi_problem {
     int rows_per_warp;    /* 4 or 8; 0 = choose */
     int use_graphs;       /* 1: capture the time loops into CUDA graphs */
     int wavelet_per_shot; /* 1: wavelet region is [nshots][nt]; 0: one [nt] */
+    int forward_only;     /* 1: no checkpoint, virtual-source or gradient memory;
+                             twi_gradient and save_checkpoints are refused */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */
@@ -192,6 +194,41 @@ int twi_batch_bind(twi_batch* batch, void* workspace, size_t bytes);
 int twi_batch_forward(twi_batch* batch, int save_checkpoints, void* stream);
 int twi_batch_gradient(twi_batch* batch, void* stream);
 int twi_batch_destroy(twi_batch* batch);
+
+/* ------------------------------------------------------------------------
+ * 4. Request engine (continuous batching)
+ *
+ * Requests are bound plans with shots, model and wavelet set: kind 0 =
+ * forward modelling (gathers), kind 1 = gradient (forward with checkpoints,
+ * residual gathers - observed, checkpointed adjoint; the observed gathers
+ * [nshots][nt][nx] are a device pointer, NULL meaning zero data).  Each tick advances every
+ * in-flight request by one time step, one launch per kernel mode for all of
+ * them; requests join and leave between ticks.  A request's result equals
+ * running its plan alone, bit for bit.  No counterpart in the reference.
+ * ------------------------------------------------------------------------ */
+
+typedef struct twi_engine twi_engine;
+
+/* max_requests: requests in flight at once (further ones wait). */
+int twi_engine_create(int order, int exact, int rows_per_warp, int max_requests,
+                      twi_engine** engine);
+int twi_engine_workspace_size(const twi_engine* engine, size_t* bytes);
+/* Device workspace for job tables and tensor maps; also allocates the pinned
+ * host staging ring on first bind. */
+int twi_engine_bind(twi_engine* engine, void* workspace, size_t bytes);
+/* Queue a request; `tag` identifies it in twi_engine_run's report.  The plan
+ * and the observed buffer must stay alive until the request is reported. */
+int twi_engine_submit(twi_engine* engine, twi_plan* plan, int kind, const float* observed,
+                      long long tag);
+/* Enqueue up to `ticks` ticks on `stream` (returns early once a request
+ * finished) and report up to max_done finished tags.  A reported request's
+ * outputs are complete once `stream` reaches this point. */
+int twi_engine_run(twi_engine* engine, int ticks, void* stream, long long* done_tags,
+                   int max_done, int* ndone);
+/* Requests in flight on the device, and submitted or finished but not yet
+ * reported. */
+int twi_engine_pending(const twi_engine* engine, int* in_flight, int* waiting);
+int twi_engine_destroy(twi_engine* engine);
 
 #ifdef __cplusplus
 }

@@ -41,7 +41,7 @@ def test_bindings_cover_header():
 def _problem(**kw):
     base = dict(order=4, nx=100, nz=50, nt=200, h=10.0, dt=1e-3, nshots=4, ckpt_interval=0,
                 exact=1, accumulate=0, shots_per_cta=0, rows_per_warp=0, use_graphs=1,
-                wavelet_per_shot=0)
+                wavelet_per_shot=0, forward_only=0)
     base.update(kw)
     return _capi.Problem(**base)
 
@@ -94,3 +94,18 @@ def test_default_checkpoint_interval_is_sqrt_2nt():
     L.twi_plan_layout(h, ctypes.byref(lay))
     assert lay.ckpt_interval == 89 and lay.nsegments == 45
     L.twi_plan_destroy(h)
+
+
+def test_forward_only_plan_is_small():
+    L = _capi.lib()
+    full = _capi.Layout()
+    st, h = _create(nt=4000, nshots=64, nx=1000, nz=300)
+    L.twi_plan_layout(h, ctypes.byref(full))
+    L.twi_plan_destroy(h)
+    fo = _capi.Layout()
+    st, h = _create(nt=4000, nshots=64, nx=1000, nz=300, forward_only=1)
+    L.twi_plan_layout(h, ctypes.byref(fo))
+    L.twi_plan_destroy(h)
+    slot = 1024 * 304 * 4
+    assert fo.workspace_bytes < (1 + 64 * 3 + 2) * slot + 2 * 64 * 4000 * 1000 * 4
+    assert full.workspace_bytes > 10 * fo.workspace_bytes

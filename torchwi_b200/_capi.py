@@ -36,7 +36,8 @@ class Problem(ctypes.Structure):
                 ("nshots", ctypes.c_int), ("ckpt_interval", ctypes.c_int),
                 ("exact", ctypes.c_int), ("accumulate", ctypes.c_int),
                 ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int),
-                ("use_graphs", ctypes.c_int), ("wavelet_per_shot", ctypes.c_int)]
+                ("use_graphs", ctypes.c_int), ("wavelet_per_shot", ctypes.c_int),
+                ("forward_only", ctypes.c_int)]
 
 
 class Layout(ctypes.Structure):
@@ -76,6 +77,13 @@ SIGNATURES = {
     "twi_batch_forward": [_vp, _i, _vp],
     "twi_batch_gradient": [_vp, _vp],
     "twi_batch_destroy": [_vp],
+    "twi_engine_create": [_i, _i, _i, _i, ctypes.POINTER(_vp)],
+    "twi_engine_workspace_size": [_vp, ctypes.POINTER(ctypes.c_size_t)],
+    "twi_engine_bind": [_vp, _vp, ctypes.c_size_t],
+    "twi_engine_submit": [_vp, _vp, _i, _vp, ctypes.c_longlong],
+    "twi_engine_run": [_vp, _i, _vp, ctypes.POINTER(ctypes.c_longlong), _i, ctypes.POINTER(_i)],
+    "twi_engine_pending": [_vp, ctypes.POINTER(_i), ctypes.POINTER(_i)],
+    "twi_engine_destroy": [_vp],
 }
 _RESTYPES = {"twi_last_error": ctypes.c_char_p}
 

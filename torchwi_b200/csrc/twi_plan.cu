@@ -29,6 +29,7 @@
 
 #include "twi_b200.h"
 #include "twi_kernels.h"
+#include "twi_plan_internal.h"
 
 using namespace twi;
 
@@ -228,10 +229,7 @@ struct twi_plan {
         return TWI_OK;
     }
 
-    struct Step {
-        StepMode mode;
-        StepArgs a;
-    };
+    using Step = TwiStep;
 
     // The forward pass as a list of time steps.
     void forward_steps(bool save, std::vector<Step>& out) const {
@@ -373,7 +371,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->dimz = p.nz + p.order;
     P->pitch = (P->dimx + kTileX - 1) / kTileX * kTileX;
     P->slot_elems = (long long)P->pitch * P->dimz;
-    P->gradient = p.ckpt_interval >= 0;   // all plans can take gradients
+    P->gradient = p.forward_only == 0;
     P->kahan = p.accumulate == 0;
     P->rz = p.rows_per_warp ? p.rows_per_warp : 4;
     int K = p.ckpt_interval;
@@ -385,10 +383,10 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     if (spc <= 0) spc = std::min(p.nshots, 4);
     P->spc = std::min(spc, p.nshots);
     P->ngroups = (p.nshots + P->spc - 1) / P->spc;
-    P->sps = 6 + 2 * (P->nseg - 1);
+    P->sps = P->gradient ? 6 + 2 * (P->nseg - 1) : 3;
     P->nslots = 1 + (long long)p.nshots * P->sps;
-    P->nvirt = (long long)p.nshots * K;
-    P->nacc = P->kahan ? P->ngroups : p.nshots;
+    P->nvirt = P->gradient ? (long long)p.nshots * K : 0;
+    P->nacc = P->gradient ? (P->kahan ? P->ngroups : p.nshots) : 0;
 
     // workspace layout
     const size_t S = p.nshots, nt = p.nt;
@@ -404,7 +402,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->off_fields = take((size_t)P->nslots * P->slot_elems * 4);
     P->off_virt = take((size_t)P->nvirt * P->slot_elems * 4);
     P->off_acc = take((size_t)P->nacc * P->slot_elems * 4);
-    P->off_comp = take(P->kahan ? (size_t)P->nacc * P->slot_elems * 4 : 0);
+    P->off_comp = take(P->kahan && P->gradient ? (size_t)P->nacc * P->slot_elems * 4 : 0);
     P->total = off;
     *out = P;
     return TWI_OK;
@@ -490,6 +488,8 @@ int twi_forward(twi_plan* P, int save_checkpoints, void* stream) {
     if (!P->have_shots || !P->have_model)
         return fail(TWI_ERR_STATE, "set shots and model before twi_forward");
     const bool save = save_checkpoints != 0;
+    if (save && !P->gradient)
+        return fail(TWI_ERR_STATE, "a forward-only plan keeps no checkpoints");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     TWI_TRY(P->run(&P->g_fwd[save ? 1 : 0], st,
                    [&](cudaStream_t s) { return P->enqueue_forward(save, s); }));
@@ -568,6 +568,37 @@ int twi_plan_destroy(twi_plan* P) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// plan operations used by the request engine (twi_engine.cu)
+// ---------------------------------------------------------------------------
+
+void plan_tensor_maps(const twi_plan* P, CUtensorMap out[3]) {
+    out[0] = P->tm_u2;
+    out[1] = P->tm_u1;
+    out[2] = P->tm_vel;
+}
+float* plan_gathers(const twi_plan* P) { return P->F(P->off_frd); }
+long long plan_gathers_elems(const twi_plan* P) {
+    return (long long)P->p.nshots * P->p.nt * P->p.nx;
+}
+void plan_steps(const twi_plan* P, int kind, std::vector<TwiStep>& out, size_t* fwd_steps) {
+    P->forward_steps(kind == 1, out);
+    *fwd_steps = out.size();
+    if (kind == 1) P->gradient_steps(out);
+}
+int plan_gradient_prologue(const twi_plan* P, cudaStream_t st) { return P->gradient_prologue(st); }
+int plan_gradient_epilogue(const twi_plan* P, cudaStream_t st) { return P->gradient_epilogue(st); }
+void plan_mark_done(twi_plan* P, int kind) { P->have_ckpt = kind == 1; }
+int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp) {
+    if (!P->ws) return fail(TWI_ERR_STATE, "bind the plan before submitting it");
+    if (kind == 1 && !P->gradient) return fail(TWI_ERR_STATE, "a forward-only plan cannot take a gradient request");
+    if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
+    if (P->p.order != order || (P->p.exact != 0) != exact ||
+        default_shape(P->rz).rows_per_warp != rows_per_warp)
+        return fail(TWI_ERR_INVALID, "plan order/arithmetic/rows_per_warp differ from the engine's");
+    return TWI_OK;
+}
 
 // ---------------------------------------------------------------------------
 // batches of plans: one launch per kernel mode and time step for all plans

@@ -20,6 +20,8 @@ Differences, all deliberate:
 
 from __future__ import annotations
 
+import dataclasses
+
 import numpy as np
 import torch
 
@@ -59,8 +61,11 @@ class Time2dForward(torch.nn.Module):
 
     def _plan_or_new(self) -> ShotPlan:
         if self._plan is None:
+            opts = self.options
+            if self.forward_only:
+                opts = dataclasses.replace(opts, forward_only=True)
             self._plan = ShotPlan(self.nx, self.ny, self.h, self.dt, self.nt, self.order, nshots=1,
-                                  options=self.options, device=self.device)
+                                  options=opts, device=self.device)
             self._plan.set_wavelet(self.w)
         return self._plan
 

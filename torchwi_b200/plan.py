@@ -32,6 +32,8 @@ class PlanOptions:
     ckpt_interval: steps between saved wavefield pairs (0 = sqrt(2 nt)).
     shots_per_cta, rows_per_warp: launch shape (0 = default).
     use_graphs:  capture the time loops into CUDA graphs.
+    forward_only: size the plan for forward modelling only (no checkpoint,
+                 virtual-source or gradient memory).
     """
 
     exact: bool = True
@@ -40,6 +42,7 @@ class PlanOptions:
     shots_per_cta: int = 0
     rows_per_warp: int = 0
     use_graphs: bool = True
+    forward_only: bool = False
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -69,7 +72,8 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    nshots=int(nshots), ckpt_interval=int(o.ckpt_interval), exact=int(bool(o.exact)),
                    accumulate=0 if o.accumulate == "kahan" else 1,
                    shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
-                   use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)))
+                   use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
+                   forward_only=int(bool(o.forward_only)))
 
 
 class ShotPlan:

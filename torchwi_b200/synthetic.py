@@ -175,3 +175,36 @@ def small_case(nx=48, nz=32, nt=300, nshots=2, order=4, seed=7, h=10.0, dt=1.0e-
     return Survey(f"small_{nx}x{nz}x{nt}_o{order}", v.astype(np.float32), h, dt,
                   ricker(freq, dt, nt).astype(np.float32), sx, sy, sy.copy(), order=order,
                   vel_start=gaussian_filter(v, 3.0).astype(np.float32))
+
+
+SERVE_GRIDS = ((500, 200), (1000, 300), (2000, 600), (4000, 1200))
+
+
+def config5(rate: float, nreq: int = 24, seed: int = 5, max_shots: int = 128,
+            nt_range=(2000, 8000), grids=SERVE_GRIDS, h: float = 10.0, dt: float = 1.0e-3):
+    """Serving stream: Poisson arrivals at `rate` req/s (seeded), forward or
+    gradient requests (50/50) on a resident pool of one layered model per grid
+    size {500x200, 1000x300, 2000x600, 4000x1200}, 1..max_shots surface shots,
+    nt uniform in nt_range, Ricker 8 Hz, h = 10 m, dt = 1 ms (CFL 0.32).
+    Returns (models {name: (nx, nz) float32}, requests [dict])."""
+    rng = np.random.default_rng(seed)
+    models = {}
+    for nx, nz in grids:
+        m = _layered(nx, nz, np.random.default_rng(seed * 1000 + nx))
+        models[f"layered_{nx}x{nz}"] = m.astype(np.float32)
+    names = list(models)
+    t = 0.0
+    reqs = []
+    for i in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        g = int(rng.integers(len(grids)))
+        nx, nz = grids[g]
+        ns = int(rng.integers(1, max_shots + 1))
+        nt = int(rng.integers(nt_range[0], nt_range[1] + 1))
+        kind = "forward" if rng.random() < 0.5 else "gradient"
+        ix = ((np.arange(ns) + 0.5) * nx / ns).astype(np.int64)
+        sx = ix.astype(np.float64) * h
+        sy = np.full(ns, 2 * h)
+        reqs.append(dict(kind=kind, model=names[g], sx=sx, sy=sy, ry=sy.copy(),
+                         w=ricker(8.0, dt, nt).astype(np.float32), arrival=t))
+    return models, reqs
