@@ -95,6 +95,17 @@ int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const float* w, i
                                  int dimx, int dimy, int nt, float h, float dt, float sx,
                                  float sy, float ry, void* stream);
 
+/* Excitation-amplitude variants, replacing the reference's td2d_exa_cuda
+ * module functions (torchwi/propagator/td2d/propagator_exa_cuda.h:2-38,
+ * wrapper_exa_cuda.cpp:9-83).  exa is [dimy][dimx] float, iexa [dimy][dimx]
+ * int16 (the step of the largest-magnitude virtual source); nt <= 32767. */
+int twi_fdm_exa_forward(float* frd, float* exa, short* iexa, float* u1, float* u2, float* u3,
+                        const float* vel, const float* w, int order, int dimx, int dimy, int nt,
+                        float h, float dt, float sx, float sy, float ry, void* stream);
+int twi_fdm_exa_backward(float* grad, const float* exa, const short* iexa, float* u1, float* u2,
+                         float* u3, const float* vel, const float* resid, int order, int dimx,
+                         int dimy, int nt, float h, float dt, float ry, void* stream);
+
 /* ------------------------------------------------------------------------
  * 2. Plan API
  *
@@ -122,6 +133,9 @@ typedef struct twi_problem {
     int wavelet_per_shot; /* 1: wavelet region is [nshots][nt]; 0: one [nt] */
     int forward_only;     /* 1: no checkpoint, virtual-source or gradient memory;
                              twi_gradient and save_checkpoints are refused */
+    int exa;              /* 1: excitation-amplitude gradient (no checkpoints): the
+                             forward pass keeps the largest virtual source per cell
+                             and its step (16-bit, nt <= 32767); plan-level calls only */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */

@@ -23,6 +23,8 @@ from .oracle import (  # noqa: F401
     ref_forward,
     ref_forward_only,
     twio_backward,
+    twio_exa_backward,
+    twio_exa_forward,
     twio_forward,
     shot_gather,
     shot_gradient,

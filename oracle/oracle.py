@@ -69,8 +69,14 @@ def _load(path: str) -> ctypes.CDLL:
                                                   _f, _f, _f, _i]
                 lib.twio_backward_f64.argtypes = [_D, _D, _D, _D, _i, _i, _i, _i,
                                                   _d, _d, _d, _i]
+                _S = ctypes.POINTER(ctypes.c_int16)
+                lib.twio_exa_forward_f32.argtypes = [_F, _F, _S, _F, _F, _i, _i, _i, _i,
+                                                     _f, _f, _f, _f, _f]
+                lib.twio_exa_backward_f32.argtypes = [_F, _F, _S, _F, _F, _i, _i, _i, _i,
+                                                      _f, _f, _f]
                 for fn in ("twio_forward_f32", "twio_forward_f64",
-                           "twio_backward_f32", "twio_backward_f64"):
+                           "twio_backward_f32", "twio_backward_f64",
+                           "twio_exa_forward_f32", "twio_exa_backward_f32"):
                     getattr(lib, fn).restype = _i
             else:
                 lib.ref_fdm_forward.argtypes = [_F] * 7 + [_i] * 4 + [_f] * 5
@@ -96,7 +102,8 @@ def _check(status: int) -> None:
     if status != 0:
         raise OracleError({1: "order must be 2, 4 or 8",
                            2: "source outside the model",
-                           3: "receiver row outside the grid"}.get(status, str(status)))
+                           3: "receiver row outside the grid",
+                           4: "nt above 32767 (16-bit step index)"}.get(status, str(status)))
 
 
 # ----------------------------------------------------------------------------
@@ -137,6 +144,31 @@ def twio_backward(virt, vpad, resid, order, dimx, dimy, nt, h, dt, ry,
     fn = lib.twio_backward_f64 if f64 else lib.twio_backward_f32
     _check(fn(_ptr(grad, kind), _ptr(virt, kind), _ptr(vpad, kind),
               _ptr(resid, kind), order, dimx, dimy, nt, h, dt, ry, int(kahan)))
+    return grad
+
+
+def twio_exa_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
+    """Excitation-amplitude forward pass: (frd[nt, nx], exa[dimxy], iexa[dimxy] int16)."""
+    lib = _load(_ORACLE_SO)
+    vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel()
+    w = np.ascontiguousarray(w, dtype=np.float32).ravel()
+    frd = np.zeros((nt, dimx - order), dtype=np.float32)
+    exa = np.zeros(dimx * dimy, dtype=np.float32)
+    iexa = np.zeros(dimx * dimy, dtype=np.int16)
+    _check(lib.twio_exa_forward_f32(_ptr(frd), _ptr(exa), iexa.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                    _ptr(vpad), _ptr(w), order, dimx, dimy, nt, h, dt, sx, sy, ry))
+    return frd, exa, iexa
+
+
+def twio_exa_backward(exa, iexa, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
+    lib = _load(_ORACLE_SO)
+    exa = np.ascontiguousarray(exa, dtype=np.float32)
+    iexa = np.ascontiguousarray(iexa, dtype=np.int16)
+    vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel()
+    resid = np.ascontiguousarray(resid, dtype=np.float32)
+    grad = np.zeros(dimx * dimy, dtype=np.float32)
+    _check(lib.twio_exa_backward_f32(_ptr(grad), _ptr(exa), iexa.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+                                     _ptr(vpad), _ptr(resid), order, dimx, dimy, nt, h, dt, ry))
     return grad
 
 

@@ -267,9 +267,95 @@ int backward_impl(T* grad, const T* virt, const T* vel, const T* resid,
     return 0;
 }
 
+// Excitation-amplitude gradient (propagator_exa_cuda.cu:5-159,
+// td2d_cuda.cu:182-205): the forward pass keeps, per cell, the virtual
+// source of largest magnitude (strictly larger replaces; ties keep the
+// earlier step) and its step index as a 16-bit integer; the adjoint pass
+// assigns grad = -exa * lambda at that step.  The reference implements this
+// on CUDA only; the stencil, Keys and virtual-source arithmetic here are
+// those of the CPU propagator, like the rest of this file.
+template <typename T>
+int exa_forward_impl(T* frd, T* exa, std::int16_t* iexa, const T* vel, const T* w, int order,
+                     int dimx, int dimy, int nt, T h, T dt, T sx, T sy, T ry) {
+    if (order != 2 && order != 4 && order != 8) return 1;
+    if (nt > 32767) return 4;
+    Grid<T> g(order, dimx, dimy, h, dt);
+    const int isx = cell_of(sx, h), isy = cell_of(sy, h), iry = cell_of(ry, h);
+    if (isx < 0 || isy < 0 || isx >= g.nx || isy >= g.ny) return 2;
+    if (iry < 0 || iry + g.ne >= dimy) return 3;
+    const std::int64_t src = static_cast<std::int64_t>(isy + g.ne) * dimx + isx + g.ne;
+    const std::int64_t rec = static_cast<std::int64_t>(iry + g.ne) * dimx + g.ne;
+    const T cons = static_cast<T>(-2.0 / static_cast<double>(g.dt2));
+    std::vector<T> buf(3 * g.dimxy, T(0));
+    T* um = buf.data();
+    T* uo = um + g.dimxy;
+    T* up = uo + g.dimxy;
+    for (std::int64_t i = 0; i < g.dimxy; ++i) exa[i] = T(0), iexa[i] = 0;
+    for (int it = 0; it < nt; ++it) {
+        g.interior(um, uo, up, vel);
+        up[src] = up[src] + w[it] * vel[src] * vel[src] * g.dt2;
+        g.keys(um, uo, up, vel);
+        std::memcpy(frd + static_cast<std::int64_t>(it) * g.nx, up + rec, sizeof(T) * g.nx);
+#pragma omp parallel for schedule(static)
+        for (std::int64_t i = 0; i < g.dimxy; ++i) {
+            const T v3 = vel[i] * vel[i] * vel[i];
+            const T vt = cons / v3 * ((um[i] - T(2) * uo[i]) + up[i]);
+            if (std::fabs(vt) > std::fabs(exa[i])) {
+                exa[i] = vt;
+                iexa[i] = static_cast<std::int16_t>(it);
+            }
+        }
+        T* t = um; um = uo; uo = up; up = t;
+    }
+    return 0;
+}
+
+template <typename T>
+int exa_backward_impl(T* grad, const T* exa, const std::int16_t* iexa, const T* vel,
+                      const T* resid, int order, int dimx, int dimy, int nt, T h, T dt, T ry) {
+    if (order != 2 && order != 4 && order != 8) return 1;
+    if (nt > 32767) return 4;
+    Grid<T> g(order, dimx, dimy, h, dt);
+    const int iry = cell_of(ry, h);
+    if (iry < 0 || iry + g.ne >= dimy) return 3;
+    const std::int64_t rec = static_cast<std::int64_t>(iry + g.ne) * dimx + g.ne;
+    std::vector<T> buf(3 * g.dimxy, T(0));
+    T* um = buf.data();
+    T* uo = um + g.dimxy;
+    T* up = uo + g.dimxy;
+    for (std::int64_t i = 0; i < g.dimxy; ++i) grad[i] = T(0);
+    for (int it = nt - 1; it >= 0; --it) {
+        g.interior(um, uo, up, vel);
+        const T* rs = resid + static_cast<std::int64_t>(it) * g.nx;
+        for (int c = 0; c < g.nx; ++c) {
+            const std::int64_t j = rec + c;
+            up[j] = up[j] + rs[c] * vel[j] * vel[j] * g.dt2;
+        }
+        g.keys(um, uo, up, vel);
+#pragma omp parallel for schedule(static)
+        for (std::int64_t i = 0; i < g.dimxy; ++i)
+            if (iexa[i] == it) grad[i] = (-exa[i]) * up[i];
+        T* t = um; um = uo; uo = up; up = t;
+    }
+    return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+int twio_exa_forward_f32(float* frd, float* exa, std::int16_t* iexa, const float* vel,
+                         const float* w, int order, int dimx, int dimy, int nt, float h, float dt,
+                         float sx, float sy, float ry) {
+    return exa_forward_impl<float>(frd, exa, iexa, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry);
+}
+
+int twio_exa_backward_f32(float* grad, const float* exa, const std::int16_t* iexa,
+                          const float* vel, const float* resid, int order, int dimx, int dimy,
+                          int nt, float h, float dt, float ry) {
+    return exa_backward_impl<float>(grad, exa, iexa, vel, resid, order, dimx, dimy, nt, h, dt, ry);
+}
+
 
 // Status codes: 0 ok, 1 bad order, 2 source outside the model, 3 receiver row
 // outside the grid.

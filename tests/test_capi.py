@@ -109,3 +109,18 @@ def test_forward_only_plan_is_small():
     slot = 1024 * 304 * 4
     assert fo.workspace_bytes < (1 + 64 * 3 + 2) * slot + 2 * 64 * 4000 * 1000 * 4
     assert full.workspace_bytes > 10 * fo.workspace_bytes
+
+
+def test_exa_plan_ignores_kahan():
+    """Excitation amplitude assigns one value per cell and shot: its plans keep
+    one gradient slot per shot whatever the accumulation switch says."""
+    L = _capi.lib()
+    sizes = []
+    for acc in (0, 1):
+        lay = _capi.Layout()
+        st, h = _create(nt=300, nshots=8, nx=70, nz=33, exa=1, accumulate=acc)
+        assert st == 0
+        L.twi_plan_layout(h, ctypes.byref(lay))
+        L.twi_plan_destroy(h)
+        sizes.append(lay.workspace_bytes)
+    assert sizes[0] == sizes[1]

@@ -37,7 +37,7 @@ class Problem(ctypes.Structure):
                 ("exact", ctypes.c_int), ("accumulate", ctypes.c_int),
                 ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int),
                 ("use_graphs", ctypes.c_int), ("wavelet_per_shot", ctypes.c_int),
-                ("forward_only", ctypes.c_int)]
+                ("forward_only", ctypes.c_int), ("exa", ctypes.c_int)]
 
 
 class Layout(ctypes.Structure):
@@ -61,6 +61,8 @@ SIGNATURES = {
     "twi_fdm_backward": [_vp] * 7 + [_i] * 4 + [_f] * 3 + [_vp],
     "twi_fdm_forward_only": [_vp] * 6 + [_i] * 4 + [_f] * 5 + [_vp],
     "twi_fdm_forward_only_noalloc": [_vp] * 3 + [_i] * 4 + [_f] * 5 + [_vp],
+    "twi_fdm_exa_forward": [_vp] * 8 + [_i] * 4 + [_f] * 5 + [_vp],
+    "twi_fdm_exa_backward": [_vp] * 8 + [_i] * 4 + [_f] * 3 + [_vp],
     "twi_plan_create": [ctypes.POINTER(Problem), ctypes.POINTER(_vp)],
     "twi_plan_layout": [_vp, ctypes.POINTER(Layout)],
     "twi_plan_bind": [_vp, _vp, ctypes.c_size_t],

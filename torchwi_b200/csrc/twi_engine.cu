@@ -8,11 +8,14 @@
 // leave between ticks, so a short request admitted while a long one runs
 // finishes after its own number of ticks, sharing the GPU with the long one.
 //
-// Ordering: everything -- job-table uploads, tensor-map uploads, launches,
-// residual and reduction kernels -- is enqueued on the stream passed to
-// twi_engine_run, so device-side reuse of a job-table or tensor-map slot is
-// ordered after the kernels that read it.  Host staging buffers are pinned
-// and reused only after the event of their last copy has completed.
+// A request's static arguments (one template per kernel mode) and tensor
+// maps are uploaded once, at admission, into fixed slots of the engine's
+// workspace; a launch carries its jobs' per-step integers and CTA offsets in
+// its kernel parameters, so ticks issue no copies.  Everything -- uploads,
+// launches, residual and reduction kernels -- is enqueued on the stream
+// passed to twi_engine_run, so reuse of a slot is ordered after the kernels
+// that read it; its pinned host staging is reused only after the event of
+// its last upload has completed.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -50,8 +53,6 @@ __global__ void residual_kernel(float* __restrict__ frd, const float* __restrict
         frd[i] = frd[i] - obs[i];
 }
 
-constexpr int kRing = 64;   // job-table slots in flight
-
 }  // namespace
 
 using namespace twi;
@@ -62,19 +63,23 @@ struct twi_engine {
     LaunchShape shape{4, 4};
     int max_requests = 0;
     char* ws = nullptr;
-    size_t off_tmaps = 0, off_ring = 0, total = 0;
-    MultiJob* staging = nullptr;        // pinned, kRing * max_requests jobs
-    cudaEvent_t events[kRing] = {};
-    std::vector<cudaEvent_t> tm_events;  // per request slot: its tensor-map upload
-    int ring_next = 0;
+    size_t off_tmaps = 0, off_tmpl = 0, total = 0;
+    // pinned staging per request slot: its tensor maps and per-mode templates
+    struct SlotStage {
+        CUtensorMap tm[3];
+        MultiJob tmpl[3];
+    };
+    SlotStage* staging = nullptr;
+    std::vector<cudaEvent_t> slot_events;   // per slot: its last upload
 
     struct Request {
         twi_plan* plan = nullptr;
         int kind = 0;                   // 0 forward, 1 gradient
         const float* observed = nullptr;
         long long tag = 0;
-        int slot = -1;                  // tensor-map slot
+        int slot = -1;                  // tensor-map / template slot
         std::vector<TwiStep> steps;     // forward steps, then gradient steps
+        int nbc[3] = {0, 0, 0}, ncta[3] = {0, 0, 0};   // per kernel mode
         size_t fwd_steps = 0, pos = 0;
         bool started = false;
     };
@@ -83,19 +88,8 @@ struct twi_engine {
     std::deque<Request> waiting;        // submitted, not yet on the device
     std::deque<long long> completed;    // finished, not yet reported
 
-    int stage_launch(const std::vector<MultiJob>& jobs, StepMode mode, long long nctas,
-                     cudaStream_t st) {
-        const int r = ring_next;
-        ring_next = (ring_next + 1) % kRing;
-        ENG_CUDA(cudaEventSynchronize(events[r]));   // staging slot r is free again
-        MultiJob* host = staging + (size_t)r * max_requests;
-        MultiJob* dev = reinterpret_cast<MultiJob*>(ws + off_ring) + (size_t)r * max_requests;
-        std::memcpy(host, jobs.data(), jobs.size() * sizeof(MultiJob));
-        ENG_CUDA(cudaMemcpyAsync(dev, host, jobs.size() * sizeof(MultiJob), cudaMemcpyHostToDevice, st));
-        ENG_CUDA(cudaEventRecord(events[r], st));
-        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
-        ENG_CUDA(launch_step_multi(order, exact, mode, shape, dev, (int)jobs.size(), nctas, tm, st));
-        return TWI_OK;
+    const MultiJob* tmpl_dev(int slot, int mode) const {
+        return reinterpret_cast<const MultiJob*>(ws + off_tmpl) + 3 * slot + mode;
     }
 
     int admit(cudaStream_t st) {
@@ -104,16 +98,30 @@ struct twi_engine {
             waiting.pop_front();
             R.slot = free_slots.back();
             free_slots.pop_back();
-            CUtensorMap tm[3];
-            plan_tensor_maps(R.plan, tm);
-            // ordered after every kernel already enqueued that read this slot
-            CUtensorMap* host = reinterpret_cast<CUtensorMap*>(staging + (size_t)kRing * max_requests) +
-                                3 * R.slot;
-            ENG_CUDA(cudaEventSynchronize(tm_events[R.slot]));   // previous upload has read it
-            std::memcpy(host, tm, sizeof(tm));
-            ENG_CUDA(cudaMemcpyAsync(ws + off_tmaps + 3 * R.slot * sizeof(CUtensorMap), host,
-                                     sizeof(tm), cudaMemcpyHostToDevice, st));
-            ENG_CUDA(cudaEventRecord(tm_events[R.slot], st));
+            // the previous upload of this slot's staging has been read
+            ENG_CUDA(cudaEventSynchronize(slot_events[R.slot]));
+            SlotStage& S = staging[R.slot];
+            plan_tensor_maps(R.plan, S.tm);
+            bool seen[3] = {false, false, false};
+            for (const TwiStep& t : R.steps) {   // static arguments per kernel mode
+                const int m = static_cast<int>(t.mode);
+                if (seen[m]) continue;
+                seen[m] = true;
+                S.tmpl[m] = MultiJob{};
+                S.tmpl[m].a = t.a;
+                S.tmpl[m].plan = R.slot;
+                R.ncta[m] = step_ctas(order, shape, t.a, &R.nbc[m]);
+                S.tmpl[m].nbc = R.nbc[m];
+                S.tmpl[m].ncta = R.ncta[m];
+                if (R.ncta[m] <= 0) return efail(TWI_ERR_INVALID, "request launch too large");
+            }
+            // enqueued on the engine's stream: ordered after every kernel that
+            // read this slot for an earlier request
+            ENG_CUDA(cudaMemcpyAsync(ws + off_tmaps + 3 * R.slot * sizeof(CUtensorMap), S.tm,
+                                     sizeof(S.tm), cudaMemcpyHostToDevice, st));
+            ENG_CUDA(cudaMemcpyAsync(const_cast<MultiJob*>(tmpl_dev(R.slot, 0)), S.tmpl,
+                                     sizeof(S.tmpl), cudaMemcpyHostToDevice, st));
+            ENG_CUDA(cudaEventRecord(slot_events[R.slot], st));
             active.push_back(std::move(R));
         }
         return TWI_OK;
@@ -136,27 +144,37 @@ struct twi_engine {
         return TWI_OK;
     }
 
+    int launch(EngineLaunch& L, StepMode m, long long nctas, cudaStream_t st) {
+        const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
+        ENG_CUDA(launch_step_engine(order, exact, m, shape, L, nctas, tm, st));
+        L.njobs = 0;
+        return TWI_OK;
+    }
+
     int tick(cudaStream_t st, std::vector<long long>& done) {
         for (Request& R : active) {
             int s = before_step(R, st);
             if (s != TWI_OK) return s;
         }
+        EngineLaunch L;
         for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
-            std::vector<MultiJob> jobs;
+            L.njobs = 0;
             long long nctas = 0;
             for (Request& R : active) {
                 if (R.pos >= R.steps.size() || R.steps[R.pos].mode != m) continue;
-                MultiJob J{};
-                J.a = R.steps[R.pos].a;
-                J.plan = R.slot;
-                J.ncta = step_ctas(order, shape, J.a, &J.nbc);
-                if (J.ncta <= 0) return efail(TWI_ERR_INVALID, "request launch too large");
-                J.cta_begin = (int)nctas;
-                nctas += J.ncta;
-                jobs.push_back(J);
+                if (L.njobs == kEngineMaxJobs) {   // full: launch and start another
+                    int s = launch(L, m, nctas, st);
+                    if (s != TWI_OK) return s;
+                    nctas = 0;
+                }
+                L.cta_begin[L.njobs] = (int)nctas;
+                L.tmpl[L.njobs] = tmpl_dev(R.slot, m);
+                L.dyn[L.njobs] = dyn_of(R.steps[R.pos].a);
+                ++L.njobs;
+                nctas += R.ncta[m];
             }
-            if (!jobs.empty()) {
-                int s = stage_launch(jobs, m, nctas, st);
+            if (L.njobs) {
+                int s = launch(L, m, nctas, st);
                 if (s != TWI_OK) return s;
             }
         }
@@ -198,7 +216,7 @@ int twi_engine_create(int order, int exact, int rows_per_warp, int max_requests,
     size_t off = 0;
     auto take = [&](size_t b) { size_t o = off; off = (off + b + 255) & ~size_t(255); return o; };
     E->off_tmaps = take((size_t)max_requests * 3 * sizeof(CUtensorMap));
-    E->off_ring = take((size_t)kRing * max_requests * sizeof(MultiJob));
+    E->off_tmpl = take((size_t)max_requests * 3 * sizeof(MultiJob));
     E->total = off;
     for (int i = max_requests - 1; i >= 0; --i) E->free_slots.push_back(i);
     *out = E;
@@ -219,14 +237,12 @@ int twi_engine_bind(twi_engine* E, void* workspace, size_t bytes) {
     if (!E->active.empty()) return efail(TWI_ERR_STATE, "engine has requests in flight");
     E->ws = static_cast<char*>(workspace);
     if (!E->staging) {
-        const size_t host_bytes = (size_t)kRing * E->max_requests * sizeof(MultiJob) +
-                                  (size_t)E->max_requests * 3 * sizeof(CUtensorMap);
         void* p = nullptr;
-        ENG_CUDA(cudaHostAlloc(&p, host_bytes, cudaHostAllocDefault));
-        E->staging = static_cast<MultiJob*>(p);
-        for (auto& ev : E->events) ENG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        E->tm_events.assign(E->max_requests, nullptr);
-        for (auto& ev : E->tm_events) ENG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        ENG_CUDA(cudaHostAlloc(&p, (size_t)E->max_requests * sizeof(twi_engine::SlotStage),
+                               cudaHostAllocDefault));
+        E->staging = static_cast<twi_engine::SlotStage*>(p);
+        E->slot_events.assign(E->max_requests, nullptr);
+        for (auto& ev : E->slot_events) ENG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     }
     return TWI_OK;
 }
@@ -279,9 +295,7 @@ int twi_engine_pending(const twi_engine* E, int* in_flight, int* waiting) {
 
 int twi_engine_destroy(twi_engine* E) {
     if (!E) return TWI_OK;
-    for (auto& ev : E->events)
-        if (ev) cudaEventSynchronize(ev), cudaEventDestroy(ev);
-    for (auto& ev : E->tm_events)
+    for (auto& ev : E->slot_events)
         if (ev) cudaEventSynchronize(ev), cudaEventDestroy(ev);
     if (E->staging) cudaFreeHost(E->staging);
     delete E;

@@ -14,6 +14,8 @@ enum StepMode : int {
     kModeRecompute = 1,   // u^{n+1}; point source; virtual source written out
     kModeAdjoint = 2,     // lambda step; adjoint source on the receiver row;
                           // gradient term accumulated
+    kModeExaForward = 3,  // forward step; the virtual source of largest
+                          // magnitude and its step index kept per cell
 };
 
 // Gradient accumulator layout used by kModeAdjoint.
@@ -21,6 +23,7 @@ enum AccMode : int {
     kAccNone = 0,
     kAccPlainPerShot = 1,   // acc[shot] += term  (reference summation order)
     kAccKahanPerGroup = 2,  // Kahan pair (acc, comp)[group] over steps and shots
+    kAccExa = 3,            // acc[shot] = -exa * lambda at the step stored in iexa
 };
 
 // Geometry: the padded grid has dimz rows of dimx cells stored with a row
@@ -61,10 +64,27 @@ struct StepArgs {
     // gradient accumulators (mode 2), same pitch/slot size as the fields
     float* acc;
     float* acc_comp;
+    // excitation amplitude (modes 3 and kAccExa): per shot, same pitch/slot size
+    float* exa;
+    short* iexa;
     int acc_mode;
     int acc_base;               // slot of group 0 / shot 0
     int* err;                   // device error word (bit 0: TMA wait timeout)
 };
+
+// The part of a time step's arguments that changes from step to step.
+struct StepDyn {
+    int it;
+    int prev_base, prev_stride;
+    int cur_base, cur_stride;
+    int next_base, next_stride;
+    int virt_base;
+};
+
+__host__ __device__ inline StepDyn dyn_of(const StepArgs& a) {
+    return StepDyn{a.it, a.prev_base, a.prev_stride, a.cur_base, a.cur_stride,
+                   a.next_base, a.next_stride, a.virt_base};
+}
 
 // One job of a multi-plan launch (device memory, 64-byte aligned).
 struct alignas(64) MultiJob {
@@ -73,6 +93,17 @@ struct alignas(64) MultiJob {
     int plan;        // index of the plan's tensor maps (3 per plan)
     int nbc;         // boundary CTAs per shot group
     int ncta;        // CTAs of this job
+};
+
+// An engine launch, passed as a kernel parameter: per job its CTA offset,
+// the device-resident template of its request and kernel mode (the static
+// arguments) and the per-step integers.
+constexpr int kEngineMaxJobs = 64;
+struct EngineLaunch {
+    int njobs;
+    int cta_begin[kEngineMaxJobs];
+    const MultiJob* tmpl[kEngineMaxJobs];
+    StepDyn dyn[kEngineMaxJobs];
 };
 
 struct LaunchShape {
@@ -96,6 +127,11 @@ cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape 
                               const MultiJob* jobs, int njobs, long long nctas,
                               const CUtensorMap* tmaps, cudaStream_t stream);
 
+// One engine launch (job entries in device memory, index in parameters).
+cudaError_t launch_step_engine(int order, bool exact, StepMode mode, LaunchShape shape,
+                               const EngineLaunch& L, long long nctas, const CUtensorMap* tmaps,
+                               cudaStream_t stream);
+
 // Set kernel attributes for all modes of (order, exact, shape) on the current
 // device.  Must run before a stream capture that launches them.
 cudaError_t prepare_step(int order, bool exact, LaunchShape shape);
@@ -109,6 +145,10 @@ __host__ __device__ constexpr int zhalo(int order) { return order / 2; }
 // and this many cells per thread, ahead of the interior tiles in the grid.
 constexpr int kBoundaryCellsPerThread = 4;
 constexpr int kThreads = 128;
+
+// Store n host integers into device memory through kernel parameters
+// (chunks of 2048), ordered on `stream` without a host synchronisation.
+cudaError_t launch_store_ints(int* dst, const int* src, int n, cudaStream_t stream);
 
 // (nx, nz) z-fastest user model -> padded [dimz][pitch] x-fastest,
 // edge-replicated by ne cells (TimeOperator.py:55-58); columns >= dimx are 0.

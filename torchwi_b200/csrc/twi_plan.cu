@@ -152,18 +152,28 @@ struct twi_plan {
     int ne = 0, dimx = 0, dimz = 0, pitch = 0;
     long long slot_elems = 0;
     int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
-    bool gradient = true, kahan = true;
+    bool gradient = true, kahan = true, exa = false;
     long long nslots = 0, nvirt = 0, nacc = 0;
     // workspace regions (byte offsets)
     size_t off_vel = 0, off_wav = 0, off_frd = 0, off_grad = 0, off_coords = 0, off_err = 0,
-           off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, total = 0;
+           off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, off_exa = 0,
+           off_iexa = 0, total = 0;
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
     cudaGraphExec_t g_bwd = nullptr;
-    bool have_ckpt = false, have_shots = false, have_model = false;
+    bool have_ckpt = false, have_shots = false, have_model = false, need_zero = false;
+
+    int clear_once(cudaStream_t st) {
+        if (!need_zero) return TWI_OK;
+        TWI_CUDA(cudaMemsetAsync(F(off_fields), 0, (size_t)slot_elems * 4, st));
+        TWI_CUDA(cudaMemsetAsync(I(off_err), 0, 4, st));
+        TWI_CUDA(cudaMemsetAsync(F(off_vpad), 0, (size_t)slot_elems * 4, st));
+        need_zero = false;
+        return TWI_OK;
+    }
 
     float* F(size_t off) const { return reinterpret_cast<float*>(ws + off); }
     int* I(size_t off) const { return reinterpret_cast<int*>(ws + off); }
@@ -176,7 +186,7 @@ struct twi_plan {
     // slot of u^k during the forward pass
     Slot fwd_slot(long long k, bool save) const {
         if (k <= 0) return zero();
-        if (save && gradient) {
+        if (save && gradient && !exa) {
             if (k % K == 0 && k / K < nseg) return ckpt((int)(k / K), 1);
             if ((k + 1) % K == 0 && (k + 1) / K < nseg) return ckpt((int)((k + 1) / K), 0);
         }
@@ -235,6 +245,11 @@ struct twi_plan {
     void forward_steps(bool save, std::vector<Step>& out) const {
         StepArgs a = base_args();
         a.frd = F(off_frd);
+        const StepMode mode = save && exa ? kModeExaForward : kModeForward;
+        if (exa) {
+            a.exa = F(off_exa);
+            a.iexa = reinterpret_cast<short*>(ws + off_iexa);
+        }
         for (int it = 0; it < p.nt; ++it) {
             const Slot pv = fwd_slot(it - 1, save), cu = fwd_slot(it, save),
                        nx_ = fwd_slot(it + 1, save);
@@ -242,13 +257,34 @@ struct twi_plan {
             a.prev_base = pv.base, a.prev_stride = pv.stride;
             a.cur_base = cu.base, a.cur_stride = cu.stride;
             a.next_base = nx_.base, a.next_stride = nx_.stride;
-            out.push_back({kModeForward, a});
+            out.push_back({mode, a});
+        }
+    }
+
+    // Excitation amplitude: nt adjoint steps assigning -exa * lambda.
+    void exa_gradient_steps(std::vector<Step>& out) const {
+        StepArgs a = base_args();
+        a.resid = F(off_frd);
+        a.acc = F(off_acc);
+        a.acc_mode = kAccExa;
+        a.acc_base = 0;
+        a.exa = F(off_exa);
+        a.iexa = reinterpret_cast<short*>(ws + off_iexa);
+        for (int it = p.nt - 1; it >= 0; --it) {
+            const long long m = (long long)p.nt - 1 - it;
+            const Slot pv = lam_slot(m - 2), cu = lam_slot(m - 1), nx_ = lam_slot(m);
+            a.it = it;
+            a.prev_base = pv.base, a.prev_stride = pv.stride;
+            a.cur_base = cu.base, a.cur_stride = cu.stride;
+            a.next_base = nx_.base, a.next_stride = nx_.stride;
+            out.push_back({kModeAdjoint, a});
         }
     }
 
     // The gradient pass (without the accumulator reset and the final
     // reduction) as a list of time steps: per segment, recompute then adjoint.
     void gradient_steps(std::vector<Step>& out) const {
+        if (exa) return exa_gradient_steps(out);
         StepArgs a = base_args();
         a.virt_out = F(off_virt);
         a.virt_in = F(off_virt);
@@ -301,6 +337,10 @@ struct twi_plan {
     }
 
     int enqueue_forward(bool save, cudaStream_t st) const {
+        if (save && exa) {   // the maxima start from zero
+            TWI_CUDA(cudaMemsetAsync(F(off_exa), 0, (size_t)p.nshots * slot_elems * 4, st));
+            TWI_CUDA(cudaMemsetAsync(ws + off_iexa, 0, (size_t)p.nshots * slot_elems * 2, st));
+        }
         std::vector<Step> steps;
         forward_steps(save, steps);
         for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st));
@@ -372,7 +412,15 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->pitch = (P->dimx + kTileX - 1) / kTileX * kTileX;
     P->slot_elems = (long long)P->pitch * P->dimz;
     P->gradient = p.forward_only == 0;
+    P->exa = p.exa != 0 && P->gradient;
+    if (P->exa && p.nt > 32767) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "excitation amplitude stores 16-bit step indices: nt <= 32767");
+    }
     P->kahan = p.accumulate == 0;
+    // excitation amplitude assigns one value per cell and shot: one slot per
+    // shot (the adjoint writes acc + s * slot), summed in shot order
+    if (P->exa) P->kahan = false;
     P->rz = p.rows_per_warp ? p.rows_per_warp : 4;
     int K = p.ckpt_interval;
     if (K == 0) K = std::max(2, (int)std::lround(std::sqrt(2.0 * p.nt)));
@@ -383,9 +431,9 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     if (spc <= 0) spc = std::min(p.nshots, 4);
     P->spc = std::min(spc, p.nshots);
     P->ngroups = (p.nshots + P->spc - 1) / P->spc;
-    P->sps = P->gradient ? 6 + 2 * (P->nseg - 1) : 3;
+    P->sps = P->exa ? 6 : P->gradient ? 6 + 2 * (P->nseg - 1) : 3;
     P->nslots = 1 + (long long)p.nshots * P->sps;
-    P->nvirt = P->gradient ? (long long)p.nshots * K : 0;
+    P->nvirt = P->gradient && !P->exa ? (long long)p.nshots * K : 0;
     P->nacc = P->gradient ? (P->kahan ? P->ngroups : p.nshots) : 0;
 
     // workspace layout
@@ -403,6 +451,8 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->off_virt = take((size_t)P->nvirt * P->slot_elems * 4);
     P->off_acc = take((size_t)P->nacc * P->slot_elems * 4);
     P->off_comp = take(P->kahan && P->gradient ? (size_t)P->nacc * P->slot_elems * 4 : 0);
+    P->off_exa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 4 : 0);
+    P->off_iexa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 2 : 0);
     P->total = off;
     *out = P;
     return TWI_OK;
@@ -443,10 +493,9 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
     TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
                      TZ));
     TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
-    // zero slot, error word and velocity padding columns
-    TWI_CUDA(cudaMemset(P->F(P->off_fields), 0, (size_t)P->slot_elems * 4));
-    TWI_CUDA(cudaMemset(P->I(P->off_err), 0, 4));
-    TWI_CUDA(cudaMemset(P->F(P->off_vpad), 0, (size_t)P->slot_elems * 4));
+    // the zero slot, error word and velocity padding columns are cleared on
+    // the caller's stream by the next set_shots / set_model
+    P->need_zero = true;
     P->have_ckpt = false;
     return TWI_OK;
 }
@@ -466,8 +515,10 @@ int twi_plan_set_shots(twi_plan* P, const float* sx, const float* sy, const floa
         c[2 * S + s] = rr;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    TWI_CUDA(cudaMemcpyAsync(P->I(P->off_coords), c.data(), c.size() * 4, cudaMemcpyHostToDevice, st));
-    TWI_CUDA(cudaStreamSynchronize(st));   // the host vector goes out of scope
+    TWI_TRY(P->clear_once(st));
+    // through kernel parameters: no copy from pageable memory, no stream sync
+    cudaError_t e = launch_store_ints(P->I(P->off_coords), c.data(), (int)c.size(), st);
+    if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("shot upload: ") + cudaGetErrorString(e));
     P->have_shots = true;
     P->have_ckpt = false;
     return TWI_OK;
@@ -475,6 +526,7 @@ int twi_plan_set_shots(twi_plan* P, const float* sx, const float* sy, const floa
 
 int twi_plan_set_model(twi_plan* P, void* stream) {
     if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    TWI_TRY(P->clear_once(static_cast<cudaStream_t>(stream)));
     cudaError_t e = launch_pad_model(P->F(P->off_vel), P->F(P->off_vpad), P->p.nx, P->p.nz, P->ne,
                                      P->dimx, P->dimz, P->pitch, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("pad: ") + cudaGetErrorString(e));
@@ -593,6 +645,7 @@ void plan_mark_done(twi_plan* P, int kind) { P->have_ckpt = kind == 1; }
 int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp) {
     if (!P->ws) return fail(TWI_ERR_STATE, "bind the plan before submitting it");
     if (kind == 1 && !P->gradient) return fail(TWI_ERR_STATE, "a forward-only plan cannot take a gradient request");
+    if (P->exa) return fail(TWI_ERR_INVALID, "excitation-amplitude plans run through twi_forward/twi_gradient only");
     if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
     if (P->p.order != order || (P->p.exact != 0) != exact ||
         default_shape(P->rz).rows_per_warp != rows_per_warp)
@@ -734,7 +787,12 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
             B->exact = P->p.exact != 0;
             B->use_graphs = P->p.use_graphs != 0;
             B->shape = default_shape(P->rz);
-        } else if (P->p.order != B->order || (P->p.exact != 0) != B->exact ||
+        }
+        if (P->exa) {
+            delete B;
+            return fail(TWI_ERR_INVALID, "excitation-amplitude plans run through twi_forward/twi_gradient only");
+        }
+        if (P->p.order != B->order || (P->p.exact != 0) != B->exact ||
                    default_shape(P->rz).rows_per_warp != B->shape.rows_per_warp) {
             delete B;
             return fail(TWI_ERR_INVALID, "plans of a batch must share order, arithmetic and rows_per_warp");
@@ -823,7 +881,7 @@ struct RefRun {
     float h, dt;
     char* scratch = nullptr;
     size_t off_vpad = 0, off_fields = 0, off_wav = 0, off_coords = 0, off_err = 0, off_acc = 0,
-           total = 0;
+           off_exa = 0, off_iexa = 0, total = 0;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
     cudaStream_t st = nullptr;
 
@@ -831,7 +889,7 @@ struct RefRun {
     int* I(size_t o) const { return reinterpret_cast<int*>(scratch + o); }
 
     int setup(int order_, int dimx_, int dimy_, int nt_, float h_, float dt_, bool with_acc,
-              cudaStream_t st_) {
+              cudaStream_t st_, bool with_exa = false) {
         TWI_TRY(check_order(order_));
         order = order_, ne = order_ / 2, dimx = dimx_, dimz = dimy_, nt = nt_, h = h_, dt = dt_;
         nx = dimx - order;
@@ -846,6 +904,8 @@ struct RefRun {
         off_vpad = take((size_t)slot_elems * 4);
         off_fields = take((size_t)4 * slot_elems * 4);   // zero slot + 3 rotating
         off_acc = take(with_acc ? (size_t)slot_elems * 4 : 0);
+        off_exa = take(with_exa ? (size_t)slot_elems * 4 : 0);
+        off_iexa = take(with_exa ? (size_t)slot_elems * 2 : 0);
         off_wav = take((size_t)nt * 4);
         off_coords = take(3 * 4);
         off_err = take(4);
@@ -949,9 +1009,101 @@ int ref_forward(float* frd, float* virt, const float* vel, const float* w, int o
     return R.finish(s);
 }
 
+int exa_check(int nt) {
+    if (nt > 32767) return fail(TWI_ERR_INVALID, "excitation amplitude stores 16-bit step indices: nt <= 32767");
+    return TWI_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int twi_fdm_exa_forward(float* frd, float* exa, short* iexa, float* u1, float* u2, float* u3,
+                        const float* vel, const float* w, int order, int dimx, int dimy, int nt,
+                        float h, float dt, float sx, float sy, float ry, void* stream) {
+    (void)u1, (void)u2, (void)u3;
+    if (!frd || !exa || !iexa || !vel || !w) return fail(TWI_ERR_INVALID, "null array");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RefRun R;
+    int s = exa_check(nt);
+    if (s == TWI_OK) s = R.setup(order, dimx, dimy, nt, h, dt, false, st, true);
+    if (s == TWI_OK) s = R.load_vel(vel);
+    int coords[3];
+    if (s == TWI_OK) s = shot_cells(sx, sy, ry, h, R.nx, R.nz, R.ne, R.dimz, &coords[0], &coords[1], &coords[2]);
+    if (s == TWI_OK && cudaMemcpyAsync(R.I(R.off_coords), coords, 12, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "coordinate upload failed");
+    if (s == TWI_OK && cudaMemcpyAsync(R.F(R.off_wav), w, (size_t)nt * 4, cudaMemcpyDefault, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "wavelet upload failed");
+    if (s == TWI_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "sync failed");
+    if (s == TWI_OK) {
+        StepArgs a = R.args();
+        a.frd = frd;
+        a.exa = R.F(R.off_exa);
+        a.iexa = reinterpret_cast<short*>(R.scratch + R.off_iexa);
+        for (int it = 0; it < nt && s == TWI_OK; ++it) {
+            const Slot pv = rot_slot(it - 1), cu = rot_slot(it), nx_ = rot_slot(it + 1);
+            a.it = it;
+            a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
+            s = R.launch(kModeExaForward, a);
+        }
+        if (s == TWI_OK &&
+            (cudaMemcpy2DAsync(exa, (size_t)dimx * 4, R.F(R.off_exa), (size_t)R.pitch * 4,
+                               (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+             cudaMemcpy2DAsync(iexa, (size_t)dimx * 2, R.scratch + R.off_iexa, (size_t)R.pitch * 2,
+                               (size_t)dimx * 2, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess))
+            s = fail(TWI_ERR_CUDA, "excitation copy failed");
+    }
+    return R.finish(s);
+}
+
+int twi_fdm_exa_backward(float* grad, const float* exa, const short* iexa, float* u1, float* u2,
+                         float* u3, const float* vel, const float* resid, int order, int dimx,
+                         int dimy, int nt, float h, float dt, float ry, void* stream) {
+    (void)u1, (void)u2, (void)u3;
+    if (!grad || !exa || !iexa || !vel || !resid) return fail(TWI_ERR_INVALID, "null array");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RefRun R;
+    int s = exa_check(nt);
+    if (s == TWI_OK) s = R.setup(order, dimx, dimy, nt, h, dt, true, st, true);
+    if (s == TWI_OK) s = R.load_vel(vel);
+    int coords[3] = {-1, -1, 0};
+    if (s == TWI_OK) {
+        const int iry = cell_of(ry, h);
+        if (!(ry >= 0.f) || iry + R.ne >= R.dimz)
+            s = fail(TWI_ERR_INVALID, "receiver row outside the grid: iry=" + std::to_string(iry));
+        coords[2] = iry + R.ne;
+    }
+    if (s == TWI_OK && cudaMemcpyAsync(R.I(R.off_coords), coords, 12, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        s = fail(TWI_ERR_CUDA, "coordinate upload failed");
+    if (s == TWI_OK &&
+        (cudaMemcpy2DAsync(R.F(R.off_exa), (size_t)R.pitch * 4, exa, (size_t)dimx * 4, (size_t)dimx * 4,
+                           dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+         cudaMemcpy2DAsync(R.scratch + R.off_iexa, (size_t)R.pitch * 2, iexa, (size_t)dimx * 2,
+                           (size_t)dimx * 2, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess))
+        s = fail(TWI_ERR_CUDA, "excitation copy failed");
+    if (s == TWI_OK && cudaStreamSynchronize(st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "sync failed");
+    if (s == TWI_OK) {
+        StepArgs a = R.args();
+        a.resid = resid;
+        a.acc = R.F(R.off_acc);
+        a.acc_mode = kAccExa;
+        a.acc_base = 0;
+        a.exa = R.F(R.off_exa);
+        a.iexa = reinterpret_cast<short*>(R.scratch + R.off_iexa);
+        for (int it = nt - 1; it >= 0 && s == TWI_OK; --it) {
+            const long long m = (long long)nt - 1 - it;
+            const Slot pv = rot_slot(m - 1), cu = rot_slot(m), nx_ = rot_slot(m + 1);
+            a.it = it;
+            a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
+            s = R.launch(kModeAdjoint, a);
+        }
+        if (s == TWI_OK &&
+            cudaMemcpy2DAsync(grad, (size_t)dimx * 4, R.F(R.off_acc), (size_t)R.pitch * 4,
+                              (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            s = fail(TWI_ERR_CUDA, "gradient copy failed");
+    }
+    return R.finish(s);
+}
 
 int twi_fdm_forward(float* frd, float* virt, float* u1, float* u2, float* u3, const float* vel,
                     const float* w, int order, int dimx, int dimy, int nt, float h, float dt,

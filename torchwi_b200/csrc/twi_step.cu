@@ -73,7 +73,7 @@ __host__ __device__ inline int boundary_cells(int order, int dimx, int dimz) {
 // one thread per cell, for every shot of the group.  Neighbours come
 // straight from the slots (L2); the interior CTAs never write these cells.
 template <int ORDER, bool EXACT, int MODE>
-__device__ __forceinline__ void boundary_part(const StepArgs& a, int b, int nbc) {
+__device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& d, int b, int nbc) {
     constexpr int NE = ORDER / 2;
     const int grp = b / nbc, part = b - grp * nbc;
     const int s0 = grp * a.spc, s1 = min(s0 + a.spc, a.nshots);
@@ -98,30 +98,43 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, int b, int nbc)
         }
         const long long cell = (long long)r * a.pitch + c;
         const float v = a.vel[cell];
-        const float q = MODE == kModeRecompute ? virt_coef<EXACT>(v, a.cons) : 0.f;
+        const float q = (MODE == kModeRecompute || MODE == kModeExaForward) ? virt_coef<EXACT>(v, a.cons) : 0.f;
         for (int s = s0; s < s1; ++s) {
-            const float* U2 = a.fields + (long long)(a.cur_base + s * a.cur_stride) * a.slot_elems + cell;
-            const float* U1 = a.fields + (long long)(a.prev_base + s * a.prev_stride) * a.slot_elems + cell;
+            const float* U2 = a.fields + (long long)(d.cur_base + s * d.cur_stride) * a.slot_elems + cell;
+            const float* U1 = a.fields + (long long)(d.prev_base + s * d.prev_stride) * a.slot_elems + cell;
             const float uo = U2[0], um = U1[0];
             const float out = keys_cell<EXACT>(uo, U2[db], U2[2 * db], um, U1[db], v, a.h2, a.dt2, a.hdt);
-            a.fields[(long long)(a.next_base + s * a.next_stride) * a.slot_elems + cell] = out;
+            a.fields[(long long)(d.next_base + s * d.next_stride) * a.slot_elems + cell] = out;
             if constexpr (MODE != kModeAdjoint) {
                 // a receiver row inside the bottom pad records Keys values
                 if (a.frd != nullptr && r == a.rec_row[s] && c >= NE && c < NE + a.nx)
-                    a.frd[(long long)s * a.frd_stride + (long long)a.it * a.nx + (c - NE)] = out;
+                    a.frd[(long long)s * a.frd_stride + (long long)d.it * a.nx + (c - NE)] = out;
             }
             if constexpr (MODE == kModeRecompute) {
-                a.virt_out[(long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                a.virt_out[(long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                            (long long)r * a.virt_pitch + c] = virt_from_coef<EXACT>(q, um, uo, out);
+            }
+            if constexpr (MODE == kModeExaForward) {
+                const float vt = virt_from_coef<EXACT>(q, um, uo, out);
+                const long long e = (long long)s * a.slot_elems + cell;
+                if (fabsf(vt) > fabsf(a.exa[e])) {
+                    a.exa[e] = vt;
+                    a.iexa[e] = static_cast<short>(d.it);
+                }
             }
             if constexpr (MODE == kModeAdjoint) {
                 // pad cells are cropped by every caller; the plain per-shot sums
                 // keep them anyway so the full-grid gradient equals the reference's
                 if (a.acc_mode == kAccPlainPerShot) {
-                    const float vt = a.virt_in[(long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                    const float vt = a.virt_in[(long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                                (long long)r * a.virt_pitch + c];
                     float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + cell;
                     *g = __fadd_rn(*g, grad_term<EXACT>(vt, out));
+                } else if (a.acc_mode == kAccExa) {
+                    const long long e = (long long)s * a.slot_elems + cell;
+                    if (a.iexa[e] == d.it)
+                        a.acc[(long long)(a.acc_base + s) * a.slot_elems + cell] =
+                            grad_term<EXACT>(a.exa[e], out);
                 }
             }
         }
@@ -135,13 +148,13 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, int b, int nbc)
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUtensorMap* tm_u1p,
                                           const CUtensorMap* tm_velp, const StepArgs& a,
-                                          const int nbc, const int cta) {
+                                          const StepDyn& d, const int nbc, const int cta) {
     using S = Smem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
 
     const int ngroups = (a.nshots + a.spc - 1) / a.spc;
     if (cta < nbc * ngroups) {
-        boundary_part<ORDER, EXACT, MODE>(a, cta, nbc);
+        boundary_part<ORDER, EXACT, MODE>(a, d, cta, nbc);
         return;
     }
     const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
@@ -179,8 +192,8 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
         mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
-        tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
-        tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, a.prev_base + s * a.prev_stride, b);
+        tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, d.cur_base + s * d.cur_stride, b);
+        tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, d.prev_base + s * d.prev_stride, b);
     };
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
@@ -208,13 +221,14 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     // per-cell constants over all shots: v*v*dt^2/h^2, and for the recompute
     // the virtual-source coefficient; v itself stays in shared memory
     float4 vvreg[RZ];
-    float4 qreg[MODE == kModeRecompute ? RZ : 1];
+    constexpr bool kVirt = MODE == kModeRecompute || MODE == kModeExaForward;
+    float4 qreg[kVirt ? RZ : 1];
 #pragma unroll
     for (int rr = 0; rr < RZ; ++rr) {
         const float4 v4 = ld4(vs + (rl0 + rr) * kTileX + 4 * lane);
         vvreg[rr] = make_float4(vv_of<EXACT>(v4.x, a.dtoh2), vv_of<EXACT>(v4.y, a.dtoh2),
                                 vv_of<EXACT>(v4.z, a.dtoh2), vv_of<EXACT>(v4.w, a.dtoh2));
-        if constexpr (MODE == kModeRecompute) {
+        if constexpr (kVirt) {
             // columns past the grid hold v = 0: keep their (never stored) coefficient finite
             qreg[rr] = make_float4(virt_coef<EXACT>(v4.x != 0.f ? v4.x : 1.f, a.cons),
                                    virt_coef<EXACT>(v4.y != 0.f ? v4.y : 1.f, a.cons),
@@ -251,20 +265,23 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         if constexpr (MODE != kModeAdjoint) {
             src_r = a.src_rc[2 * s];
             src_c = a.src_rc[2 * s + 1];
-            wamp = a.wav[(long long)s * a.wav_stride + a.it];
+            wamp = a.wav[(long long)s * a.wav_stride + d.it];
         }
         const int rec_r = a.rec_row[s];
 
-        // virtual source of this step for the warp's rows (adjoint)
+        // virtual source of this step for the warp's rows (adjoint); only the
+        // virtual-source accumulations read it -- the excitation-amplitude
+        // adjoint has no virt_in array at all
         float4 vin[MODE == kModeAdjoint ? RZ : 1];
         if constexpr (MODE == kModeAdjoint) {
+            const bool need_vin = a.acc_mode == kAccKahanPerGroup || a.acc_mode == kAccPlainPerShot;
             const float* vbase =
-                a.virt_in + (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems;
+                a.virt_in + (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems;
 #pragma unroll
             for (int rr = 0; rr < RZ; ++rr) {
                 const int r = z0 + rl0 + rr;
                 vin[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (col_ok && r < a.dimz) {
+                if (need_vin && col_ok && r < a.dimz) {
                     const float* p = vbase + (long long)r * a.virt_pitch + c;
                     if (a.virt_vec4) {
                         vin[rr] = ld4(p);
@@ -314,12 +331,26 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             }
             const float4 um4 = ld4(u1s + rl * kTileX + 4 * lane);
             const float um[4] = {um4.x, um4.y, um4.z, um4.w};
-            float* dst = a.fields + (long long)(a.next_base + s * a.next_stride) * a.slot_elems +
+            float* dst = a.fields + (long long)(d.next_base + s * d.next_stride) * a.slot_elems +
                          (long long)r * a.pitch + c;
 
             if (r < NE) {
                 // free surface: the top rows stay zero (the reference never writes them)
                 if (col_ok) *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+                if constexpr (MODE == kModeAdjoint) {
+                    // the excitation-amplitude assignment covers every cell of the
+                    // grid, these rows and their corner pad cells included
+                    // (td2d_cuda.cu:197-205): -exa * 0 there
+                    if (a.acc_mode == kAccExa && col_ok) {
+                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                   (long long)r * a.pitch + c;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m < a.dimx && a.iexa[e0 + m] == d.it)
+                                g[m] = grad_term<EXACT>(a.exa[e0 + m], 0.f);
+                    }
+                }
                 if constexpr (MODE == kModeRecompute) {
                     if (col_ok) {
                         float vo[4];
@@ -327,7 +358,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         for (int m = 0; m < 4; ++m)
                             vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
                         float* p = a.virt_out +
-                                   (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                   (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                    (long long)r * a.virt_pitch + c;
                         if (a.virt_vec4) {
                             *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
@@ -367,7 +398,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     if (r == rec_r) {
                         const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
                         const float* rs =
-                            a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
+                            a.resid + (long long)s * a.resid_stride + (long long)d.it * a.nx;
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
                             const int cc = c + m;
@@ -388,7 +419,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
 
                 if constexpr (MODE != kModeAdjoint) {
                     if (a.frd != nullptr && r == rec_r) {
-                        float* g = a.frd + (long long)s * a.frd_stride + (long long)a.it * a.nx;
+                        float* g = a.frd + (long long)s * a.frd_stride + (long long)d.it * a.nx;
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
                             const int cc = c + m;
@@ -403,7 +434,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     for (int m = 0; m < 4; ++m)
                         vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
                     float* p = a.virt_out +
-                               (long long)(a.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                               (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                (long long)r * a.virt_pitch + c;
                     if (cols_interior && a.virt_vec4) {
                         *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
@@ -414,8 +445,48 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     }
                 }
 
+                if constexpr (MODE == kModeExaForward) {
+                    const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                    float4 ev = ld4(a.exa + e0);
+                    short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                    bool changed = false;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        if (!cell_in[m]) continue;
+                        const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                        if (fabsf(vt) > fabsf(comp(ev, m))) {
+                            set_comp(ev, m, vt);
+                            if (m == 0) iv.x = static_cast<short>(d.it);
+                            else if (m == 1) iv.y = static_cast<short>(d.it);
+                            else if (m == 2) iv.z = static_cast<short>(d.it);
+                            else iv.w = static_cast<short>(d.it);
+                            changed = true;
+                        }
+                    }
+                    if (changed) {
+                        if (cols_interior) {
+                            *reinterpret_cast<float4*>(a.exa + e0) = ev;
+                            *reinterpret_cast<short4*>(a.iexa + e0) = iv;
+                        } else {   // pad columns belong to the boundary CTAs
+                            const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+#pragma unroll
+                            for (int m = 0; m < 4; ++m)
+                                if (cell_in[m]) a.exa[e0 + m] = comp(ev, m), a.iexa[e0 + m] = is[m];
+                        }
+                    }
+                }
+
                 if constexpr (MODE == kModeAdjoint) {
-                    if (a.acc_mode == kAccKahanPerGroup) {
+                    if (a.acc_mode == kAccExa) {
+                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                        const short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                        const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                   (long long)r * a.pitch + c;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (cell_in[m] && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
+                    } else if (a.acc_mode == kAccKahanPerGroup) {
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
                             if (cell_in[m]) {
@@ -474,7 +545,8 @@ __global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
             const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ StepArgs a,
             const int nbc) {
-    step_body<ORDER, EXACT, MODE, RZ, WZ>(&tm_u2, &tm_u1, &tm_vel, a, nbc, blockIdx.x);
+    const StepDyn d = dyn_of(a);
+    step_body<ORDER, EXACT, MODE, RZ, WZ>(&tm_u2, &tm_u1, &tm_vel, a, d, nbc, blockIdx.x);
 }
 
 // Several plans (different grids, shots, time indices) in one launch: CTA
@@ -492,7 +564,26 @@ step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
     }
     const MultiJob& J = jobs[lo];
     const CUtensorMap* tm = tmaps + 3 * J.plan;
-    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, J.nbc, blockIdx.x - J.cta_begin);
+    const StepDyn d = dyn_of(J.a);
+    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, d, J.nbc, blockIdx.x - J.cta_begin);
+}
+
+// Engine launches: the CTA ranges and the per-step integers come from the
+// kernel parameters, the static arguments of each request and kernel mode
+// from a template resident in device memory.
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+step_kernel_engine(const __grid_constant__ EngineLaunch L, const CUtensorMap* __restrict__ tmaps) {
+    int lo = 0, hi = L.njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (L.cta_begin[mid] <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const MultiJob& J = *L.tmpl[lo];
+    const CUtensorMap* tm = tmaps + 3 * J.plan;
+    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, L.dyn[lo], J.nbc,
+                                          blockIdx.x - L.cta_begin[lo]);
 }
 
 // ---------------------------------------------------------------------------
@@ -511,6 +602,7 @@ struct LaunchReq {
     int njobs = 0;
     long long nctas = 0;
     const CUtensorMap* tmaps = nullptr;
+    const EngineLaunch* engine = nullptr;
     bool multi = false;
     bool configure_only = false;
 };
@@ -540,8 +632,13 @@ cudaError_t configure_one() {
     e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+    if constexpr (MODE != kModeExaForward) {   // multi-plan kernels: modes 0-2
+        e = cudaFuncSetAttribute(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(step_kernel_engine<ORDER, EXACT, MODE, RZ, WZ>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+    }
     if (e == cudaSuccess) configured |= 1ull << dev;
     return e;
 }
@@ -551,10 +648,18 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     using S = Smem<ORDER, RZ, WZ>;
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
     if (e != cudaSuccess || q.configure_only) return e;
-    if (q.multi) {
-        if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
-        step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>
-            <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.njobs, q.tmaps);
+    if (q.engine || q.multi) {
+        if constexpr (MODE == kModeExaForward) {
+            return cudaErrorInvalidValue;   // excitation amplitude: single-plan launches only
+        } else {
+            if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+            if (q.engine)
+                step_kernel_engine<ORDER, EXACT, MODE, RZ, WZ>
+                    <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(*q.engine, q.tmaps);
+            else
+                step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>
+                    <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.njobs, q.tmaps);
+        }
     } else {
         int nbc = 0;
         const int n = ctas_of<ORDER, RZ, WZ>(*q.a, &nbc);
@@ -578,6 +683,7 @@ cudaError_t launch_mode(StepMode mode, LaunchShape sh, const LaunchReq& q, cudaS
         case kModeForward: return launch_shape<ORDER, EXACT, kModeForward>(sh, q, st);
         case kModeRecompute: return launch_shape<ORDER, EXACT, kModeRecompute>(sh, q, st);
         case kModeAdjoint: return launch_shape<ORDER, EXACT, kModeAdjoint>(sh, q, st);
+        case kModeExaForward: return launch_shape<ORDER, EXACT, kModeExaForward>(sh, q, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -626,6 +732,15 @@ __global__ void pad_model_kernel(const float* __restrict__ vel, float* __restric
         if (row < dimz && col < pitch)
             vpad[(long long)row * pitch + col] = col < dimx ? tile[tx][rl] : 0.f;
     }
+}
+
+struct IntChunk {
+    int n;
+    int v[2048];
+};
+
+__global__ void store_ints_kernel(int* __restrict__ dst, const __grid_constant__ IntChunk c) {
+    for (int i = threadIdx.x; i < c.n; i += blockDim.x) dst[i] = c.v[i];
 }
 
 __global__ void reduce_grad_kernel(const float* __restrict__ acc, const float* __restrict__ comp,
@@ -682,6 +797,14 @@ cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape 
     return launch_req(order, exact, mode, shape, q, stream);
 }
 
+cudaError_t launch_step_engine(int order, bool exact, StepMode mode, LaunchShape shape,
+                               const EngineLaunch& L, long long nctas, const CUtensorMap* tmaps,
+                               cudaStream_t stream) {
+    LaunchReq q;
+    q.engine = &L, q.nctas = nctas, q.tmaps = tmaps;
+    return launch_req(order, exact, mode, shape, q, stream);
+}
+
 int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
     const bool r8 = shape.rows_per_warp == 8;
     switch (order) {
@@ -695,7 +818,7 @@ int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
 cudaError_t prepare_step(int order, bool exact, LaunchShape shape) {
     LaunchReq q;
     q.configure_only = true;
-    for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
+    for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeExaForward}) {
         cudaError_t e = launch_req(order, exact, m, shape, q, nullptr);
         if (e != cudaSuccess) return e;
     }
@@ -707,6 +830,18 @@ cudaError_t launch_pad_model(const float* vel_user, float* vpad, int nx, int nz,
     dim3 grid((pitch + 31) / 32, (dimz + 31) / 32);
     pad_model_kernel<<<grid, dim3(32, 8), 0, stream>>>(vel_user, vpad, nx, nz, ne, dimx, dimz, pitch);
     return cudaGetLastError();
+}
+
+cudaError_t launch_store_ints(int* dst, const int* src, int n, cudaStream_t stream) {
+    IntChunk c;
+    for (int off = 0; off < n; off += 2048) {
+        c.n = n - off < 2048 ? n - off : 2048;
+        for (int i = 0; i < c.n; ++i) c.v[i] = src[off + i];
+        store_ints_kernel<<<1, 256, 0, stream>>>(dst + off, c);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_reduce_grad(const float* acc, const float* acc_comp, int nacc,

@@ -44,27 +44,6 @@ def get_operator(device, prop="ext", exa=False, forward_only=False):
 
         return TimeForwardOperator.apply
 
-    if exa:
-
-        class TimeEXAOperator(torch.autograd.Function):
-            @staticmethod
-            def forward(ctx, vel, args):
-                sx, sy, ry, m = args
-                ex = m._exa_forward(vel, sx, sy, ry)
-                ctx.m = m
-                ctx.save_for_backward(vel.detach())
-                ctx.coords = (sx, sy, ry)
-                ctx.token = ex.token
-                return ex.gathers[0].clone()
-
-            @staticmethod
-            def backward(ctx, grad_output):
-                (vel,) = ctx.saved_tensors
-                g = ctx.m._exa_backward(vel, ctx.coords, ctx.token, grad_output)
-                return g, None
-
-        return TimeEXAOperator.apply
-
     class TimeOperator(torch.autograd.Function):
         @staticmethod
         def forward(ctx, vel, args):

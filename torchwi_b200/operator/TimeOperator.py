@@ -87,25 +87,11 @@ class Time2d(Time2dForward):
 
     def __init__(self, nx, ny, h, w, dt, order, device, prop="ext", exa=False,
                  options: PlanOptions | None = None):
+        if exa:   # excitation-amplitude gradient (TimeFunction.py:62-104)
+            options = dataclasses.replace(options or PlanOptions(), exa=True)
         super().__init__(nx, ny, h, w, dt, order, device, options)
         self.exa = bool(exa)
         self.time_modeling = TimeFunction.get_operator(self.device, prop, exa)
-
-    # excitation-amplitude mode (exa=True) -------------------------------------
-    def _exa_forward(self, vel, sx, sy, ry):
-        from ..exa import ExaPlan
-        if self._exa is None:
-            self._exa = ExaPlan(self.nx, self.ny, self.h, self.dt, self.nt, self.order,
-                                options=self.options, device=self.device)
-            self._exa.set_wavelet(self.w)
-        self._exa.run_forward(vel, _scalar(sx), _scalar(sy), _scalar(ry))
-        return self._exa
-
-    def _exa_backward(self, vel, coords, token, grad_output):
-        ex = self._exa
-        if ex.token != token:
-            ex.run_forward(vel, *(_scalar(c) for c in coords))
-        return ex.run_backward(grad_output).clone()
 
 
 class Time2dBatch(torch.nn.Module):

@@ -34,6 +34,10 @@ class PlanOptions:
     use_graphs:  capture the time loops into CUDA graphs.
     forward_only: size the plan for forward modelling only (no checkpoint,
                  virtual-source or gradient memory).
+    exa:         excitation-amplitude gradient (the reference's exa=True mode):
+                 no checkpoints; the forward pass keeps the largest virtual
+                 source per cell and its step, the adjoint assigns
+                 -exa*lambda at that step.  nt <= 32767.
     """
 
     exact: bool = True
@@ -43,6 +47,7 @@ class PlanOptions:
     rows_per_warp: int = 0
     use_graphs: bool = True
     forward_only: bool = False
+    exa: bool = False
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -73,7 +78,7 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    accumulate=0 if o.accumulate == "kahan" else 1,
                    shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
                    use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
-                   forward_only=int(bool(o.forward_only)))
+                   forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)))
 
 
 class ShotPlan:
