@@ -31,6 +31,7 @@ sys.path.insert(0, REPO)
 NX, NZ, NT, NSHOTS = 1000, 300, 4000, 64
 ALG_BYTES = {0: 16, 1: 20, 2: 28}      # per cell-update: forward, recompute, adjoint
 MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjoint step (+gradient)"}
+TRAFFIC_SHOTS = 64                      # shots per launch of the captures in profiles/traffic.json
 
 
 def _peak_hbm():
@@ -265,12 +266,16 @@ def run_b200(args):
     cells = NSHOTS * NX * NZ
     achieved = ALG_BYTES[dom] * cells / (ms_launch[dom] / 1e3) / 1e9
     peak, peak_kind = _peak_hbm()
+    # DRAM bytes per launch from one ncu capture of each mode at 64 shots on
+    # this grid; a launch's traffic grows with the shots it processes, so
+    # other shot counts scale it by NSHOTS / 64
     traffic = None
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(str(dom))
+                t64 = json.load(f).get(str(dom))
+            traffic = t64 * NSHOTS / TRAFFIC_SHOTS if t64 is not None else None
         except Exception:
             traffic = None
 
@@ -330,6 +335,8 @@ def run_b200(args):
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
+                         "traffic_source": "ncu dram__bytes_read+write per launch at "
+                                           f"{TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}",
                          "ms_per_launch": {MODE_NAMES[m]: v for m, v in ms_launch.items()}},
             "plain_form": plain,
             "cpu_baseline": cpu,
