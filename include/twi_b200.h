@@ -168,6 +168,15 @@ int twi_plan_set_model(twi_plan* plan, void* stream);
 /* Forward pass for all shots: gathers -> `gathers`.  With save_checkpoints
  * the wavefield pairs needed by twi_gradient are kept. */
 int twi_forward(twi_plan* plan, int save_checkpoints, void* stream);
+/* Forward pass with checkpoints that writes the L2 residual instead of the
+ * gathers: resid[s][it][ix] = modelled - observed[s][it][ix] (one FP32
+ * subtraction, the same bits as the reference driver's `frd - true`), and
+ * *misfit = 0.5 * sum(resid^2) accumulated in FP64 in a fixed order
+ * (examples/time/inv_torch.py:133-136, where torch forms the residual and
+ * misfit after the gathers come back).  `observed` is a device array
+ * laid out like `gathers`; `misfit` is one device double.  Follow with
+ * twi_gradient. */
+int twi_forward_residual(twi_plan* plan, const float* observed, double* misfit, void* stream);
 /* Adjoint pass for all shots from the `resid` region: recomputes the
  * forward field segment by segment from the checkpoints and writes the
  * shot-summed velocity gradient to `grad`. */

@@ -50,6 +50,8 @@ struct StepArgs {
     const int* rec_row;
     float* frd;                 // gathers (mode 0, may be null)
     long long frd_stride;       // frd[s*frd_stride + it*nx + ix]
+    const float* obs;           // observed gathers, same layout as frd: when set,
+                                // frd receives the residual modelled - observed
     // adjoint source (mode 2)
     const float* resid;
     long long resid_stride;     // resid[s*resid_stride + it*nx + ix]
@@ -158,6 +160,12 @@ cudaError_t launch_pad_model(const float* vel_user, float* vpad, int nx, int nz,
 // Combine gradient accumulators and write the (nx, nz) z-fastest result:
 // plain mode sums slots 0..nacc-1 in order; Kahan mode adds every slot's
 // (sum, -comp) pair with compensation.
+// misfit = 0.5 * sum(r[i]^2) over n samples, FP64, in a fixed order (the
+// same bits on every call); `partial` holds kMisfitBlocks doubles of scratch.
+constexpr int kMisfitBlocks = 592;
+cudaError_t launch_misfit(const float* r, long long n, double* partial, double* misfit,
+                          cudaStream_t stream);
+
 cudaError_t launch_reduce_grad(const float* acc, const float* acc_comp, int nacc,
                                long long slot_elems, int pitch, int ne, int nx, int nz,
                                int kahan, float* grad_user, cudaStream_t stream);

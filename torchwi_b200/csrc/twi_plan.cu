@@ -157,13 +157,17 @@ struct twi_plan {
     // workspace regions (byte offsets)
     size_t off_vel = 0, off_wav = 0, off_frd = 0, off_grad = 0, off_coords = 0, off_err = 0,
            off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, off_exa = 0,
-           off_iexa = 0, total = 0;
+           off_iexa = 0, off_mpart = 0, total = 0;
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
     cudaGraphExec_t g_bwd = nullptr;
+    // forward with residual: graph captured for one (observed, misfit) pair
+    cudaGraphExec_t g_fwd_res = nullptr;
+    const float* res_obs = nullptr;
+    double* res_misfit = nullptr;
     bool have_ckpt = false, have_shots = false, have_model = false, need_zero = false;
 
     int clear_once(cudaStream_t st) {
@@ -336,14 +340,25 @@ struct twi_plan {
         return TWI_OK;
     }
 
-    int enqueue_forward(bool save, cudaStream_t st) const {
+    // `obs` / `misfit` (both or neither): the gathers region receives the
+    // residual modelled - observed and *misfit = 0.5 * sum(residual^2).
+    int enqueue_forward(bool save, cudaStream_t st, const float* obs = nullptr,
+                        double* misfit = nullptr) const {
         if (save && exa) {   // the maxima start from zero
             TWI_CUDA(cudaMemsetAsync(F(off_exa), 0, (size_t)p.nshots * slot_elems * 4, st));
             TWI_CUDA(cudaMemsetAsync(ws + off_iexa, 0, (size_t)p.nshots * slot_elems * 2, st));
         }
         std::vector<Step> steps;
         forward_steps(save, steps);
-        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st));
+        for (Step& s : steps) {
+            s.a.obs = obs;
+            TWI_TRY(launch(s.mode, s.a, st));
+        }
+        if (misfit) {
+            cudaError_t e = launch_misfit(F(off_frd), (long long)p.nshots * p.nt * p.nx,
+                                          reinterpret_cast<double*>(ws + off_mpart), misfit, st);
+            if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("misfit: ") + cudaGetErrorString(e));
+        }
         return TWI_OK;
     }
 
@@ -359,6 +374,7 @@ struct twi_plan {
         for (auto& g : g_fwd)
             if (g) cudaGraphExecDestroy(g), g = nullptr;
         if (g_bwd) cudaGraphExecDestroy(g_bwd), g_bwd = nullptr;
+        if (g_fwd_res) cudaGraphExecDestroy(g_fwd_res), g_fwd_res = nullptr;
     }
 
     // Run `enqueue` directly, or capture it once into a graph and replay.
@@ -453,6 +469,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->off_comp = take(P->kahan && P->gradient ? (size_t)P->nacc * P->slot_elems * 4 : 0);
     P->off_exa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 4 : 0);
     P->off_iexa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 2 : 0);
+    P->off_mpart = take(P->gradient ? (size_t)kMisfitBlocks * sizeof(double) : 0);
     P->total = off;
     *out = P;
     return TWI_OK;
@@ -546,6 +563,25 @@ int twi_forward(twi_plan* P, int save_checkpoints, void* stream) {
     TWI_TRY(P->run(&P->g_fwd[save ? 1 : 0], st,
                    [&](cudaStream_t s) { return P->enqueue_forward(save, s); }));
     P->have_ckpt = save;
+    return TWI_OK;
+}
+
+int twi_forward_residual(twi_plan* P, const float* observed, double* misfit, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!P->have_shots || !P->have_model)
+        return fail(TWI_ERR_STATE, "set shots and model before twi_forward_residual");
+    if (!P->gradient) return fail(TWI_ERR_STATE, "a forward-only plan keeps no checkpoints");
+    if (!observed || !misfit) return fail(TWI_ERR_INVALID, "observed and misfit must not be null");
+    if (P->g_fwd_res && (P->res_obs != observed || P->res_misfit != misfit)) {
+        cudaGraphExecDestroy(P->g_fwd_res);
+        P->g_fwd_res = nullptr;
+    }
+    P->res_obs = observed;
+    P->res_misfit = misfit;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TWI_TRY(P->run(&P->g_fwd_res, st,
+                   [&](cudaStream_t s) { return P->enqueue_forward(true, s, observed, misfit); }));
+    P->have_ckpt = true;
     return TWI_OK;
 }
 

@@ -107,8 +107,10 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
             a.fields[(long long)(d.next_base + s * d.next_stride) * a.slot_elems + cell] = out;
             if constexpr (MODE != kModeAdjoint) {
                 // a receiver row inside the bottom pad records Keys values
-                if (a.frd != nullptr && r == a.rec_row[s] && c >= NE && c < NE + a.nx)
-                    a.frd[(long long)s * a.frd_stride + (long long)d.it * a.nx + (c - NE)] = out;
+                if (a.frd != nullptr && r == a.rec_row[s] && c >= NE && c < NE + a.nx) {
+                    const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx + (c - NE);
+                    a.frd[o] = a.obs != nullptr ? __fsub_rn(out, a.obs[o]) : out;
+                }
             }
             if constexpr (MODE == kModeRecompute) {
                 a.virt_out[(long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
@@ -419,11 +421,21 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
 
                 if constexpr (MODE != kModeAdjoint) {
                     if (a.frd != nullptr && r == rec_r) {
-                        float* g = a.frd + (long long)s * a.frd_stride + (long long)d.it * a.nx;
+                        const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
+                        float* g = a.frd + o;
+                        if (a.obs != nullptr) {   // the residual, one rounding like frd - obs
+                            const float* ob = a.obs + o;
 #pragma unroll
-                        for (int m = 0; m < 4; ++m) {
-                            const int cc = c + m;
-                            if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                            for (int m = 0; m < 4; ++m) {
+                                const int cc = c + m;
+                                if (cc >= NE && cc < NE + a.nx) g[cc - NE] = __fsub_rn(out[m], ob[cc - NE]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int m = 0; m < 4; ++m) {
+                                const int cc = c + m;
+                                if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                            }
                         }
                     }
                 }
@@ -779,7 +791,56 @@ __global__ void reduce_grad_kernel(const float* __restrict__ acc, const float* _
     }
 }
 
+// Misfit, pass 1: a fixed grid of kMisfitBlocks blocks; block b sums, in
+// FP64, the squares of the float4 groups b, b + grid, ... (thread-strided,
+// then a fixed tree), so the result does not depend on timing.
+__global__ void __launch_bounds__(256) misfit_partial_kernel(const float* __restrict__ r, long long n,
+                                                             double* __restrict__ partial) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    const long long n4 = n / 4;
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    for (long long i = (long long)blockIdx.x * 256 + threadIdx.x; i < n4; i += (long long)gridDim.x * 256) {
+        const float4 v = r4[i];
+        acc += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < n - 4 * n4) {
+        const double v = r[4 * n4 + threadIdx.x];
+        acc += v * v;
+    }
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
+}
+
+// Misfit, pass 2: one block adds the partial sums in a fixed order.
+__global__ void __launch_bounds__(256) misfit_final_kernel(const double* __restrict__ partial, int np,
+                                                           double* __restrict__ misfit) {
+    __shared__ double sh[256];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < np; i += 256) acc += partial[i];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *misfit = 0.5 * sh[0];
+}
+
 }  // namespace
+
+cudaError_t launch_misfit(const float* r, long long n, double* partial, double* misfit,
+                          cudaStream_t stream) {
+    if (reinterpret_cast<uintptr_t>(r) % 16 != 0) return cudaErrorMisalignedAddress;
+    misfit_partial_kernel<<<kMisfitBlocks, 256, 0, stream>>>(r, n, partial);
+    misfit_final_kernel<<<1, 256, 0, stream>>>(partial, kMisfitBlocks, misfit);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
                         const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,

@@ -70,9 +70,7 @@ def plan_local_fn(make_plan: Callable[[slice], object], observed: torch.Tensor):
             cache[key] = make_plan(shots)
         plan = cache[key]
         plan.set_model(vel)
-        frd = plan.forward(save_checkpoints=True)
-        frd.sub_(observed[shots])
-        misfit = 0.5 * frd.square().sum()
+        misfit = plan.forward_residual(observed[shots])   # residual + misfit on the device
         return misfit, plan.gradient(None).clone()
 
     return fn

@@ -157,6 +157,26 @@ class ShotPlan:
         self._have_ckpt = bool(save_checkpoints)
         return self.gathers
 
+    def forward_residual(self, observed: torch.Tensor, misfit: torch.Tensor | None = None) -> torch.Tensor:
+        """Forward pass with checkpoints that leaves the residual
+        modelled - observed in the resid region (observed [nshots, nt, nx],
+        float32, on this plan's device) and returns the misfit
+        0.5*sum(residual^2) as a 0-d float64 device tensor (written into
+        `misfit` when given).  Follow with gradient(None)."""
+        if observed.device != self.device or observed.dtype != torch.float32 or not observed.is_contiguous():
+            raise _capi.TwiInvalid(_capi.TWI_ERR_INVALID,
+                                   "observed must be a contiguous float32 tensor on the plan's device")
+        if observed.numel() != self.gathers.numel():
+            raise _capi.TwiInvalid(_capi.TWI_ERR_INVALID, f"observed must hold {tuple(self.gathers.shape)} samples")
+        if misfit is None:
+            misfit = torch.empty((), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_forward_residual(self._h, ctypes.c_void_p(observed.data_ptr()),
+                                                 ctypes.c_void_p(misfit.data_ptr()), _stream_handle()))
+        self._have_ckpt = True
+        self._keep_obs = observed   # the captured graph reads it
+        return misfit
+
     def gradient(self, resid: torch.Tensor | None = None) -> torch.Tensor:
         """Adjoint pass from `resid` [nshots, nt, nx] (already in the resid
         region when None); returns the (nx, nz) gradient view."""
