@@ -29,7 +29,7 @@ from typing import Callable
 import torch
 
 from .dist import ShardedGradient, shard_shots
-from .plan import PlanOptions, ShotPlan, footprint_bytes
+from .plan import PlanOptions, ShotPlan, shot_blocks
 
 
 # ----------------------------------------------------------------------------
@@ -131,13 +131,13 @@ def make_optimizer(params, name: str = "adam", lr: float = 0.02, momentum: float
 
 def plan_residual_local_fn(nx, nz, h, dt, w, order, sx, sy, ry, observed: torch.Tensor,
                            options: PlanOptions | None = None, device=None,
-                           hbm_budget: int | None = None) -> Callable:
+                           hbm_budget: int | None = None, observed_first: int = 0) -> Callable:
     """`local_fn(vel, shots) -> (misfit, gradient)` for `ShardedGradient`:
     the shots of the block run through batched plans (as many shots per plan
     as fit `hbm_budget`, default 80 % of free device memory), the residual
     and misfit formed on the device by the forward pass.  `observed` holds the
-    gathers of ALL shots [nshots, nt, nx] on `device` (only the block's rows
-    are read)."""
+    gathers [n, nt, nx] of shots observed_first .. observed_first+n-1 on
+    `device` (all shots, or just this rank's block)."""
     opts = options or PlanOptions()
     dev = torch.device(device) if device is not None else observed.device
     nt = int(w.numel()) if isinstance(w, torch.Tensor) else len(w)
@@ -147,21 +147,12 @@ def plan_residual_local_fn(nx, nz, h, dt, w, order, sx, sy, ry, observed: torch.
         key = (shots.start, shots.stop)
         if key in plans:
             return plans[key]
-        budget = hbm_budget
-        if budget is None:
-            free, _ = torch.cuda.mem_get_info(dev)
-            budget = int(free * 0.8)
-        n = shots.stop - shots.start
-        per = n
-        while per > 1 and footprint_bytes(nx, nz, nt, per, order, options=opts) > budget:
-            per = (per + 1) // 2
         out = []
-        for a in range(shots.start, shots.stop, per):
-            b = min(a + per, shots.stop)
-            p = ShotPlan(nx, nz, h, dt, nt, order, nshots=b - a, options=opts, device=dev)
+        for sl in shot_blocks(shots, nx, nz, nt, order, opts, hbm_budget, dev):
+            p = ShotPlan(nx, nz, h, dt, nt, order, nshots=sl.stop - sl.start, options=opts, device=dev)
             p.set_wavelet(torch.as_tensor(w))
-            p.set_shots(sx[a:b], sy[a:b], ry[a:b])
-            out.append((slice(a, b), p))
+            p.set_shots(sx[sl], sy[sl], ry[sl])
+            out.append((sl, p))
         plans[key] = out
         return out
 
@@ -170,7 +161,7 @@ def plan_residual_local_fn(nx, nz, h, dt, w, order, sx, sy, ry, observed: torch.
         misfit = torch.zeros((), dtype=torch.float64, device=dev)
         for sl, p in chunks(shots):
             p.set_model(vel)
-            misfit += p.forward_residual(observed[sl])
+            misfit += p.forward_residual(observed[sl.start - observed_first:sl.stop - observed_first])
             g = p.gradient(None)
             grad = g.clone() if grad is None else grad.add_(g)
         return misfit, grad
@@ -190,7 +181,8 @@ class Inversion:
                  h=None, dt=None, w=None, order=4, sx=None, sy=None, ry=None, observed=None,
                  vmin=None, vmax=None, parameter: str = "velocity", optimizer: str = "adam",
                  lr: float = 0.02, momentum: float = 0.9, grad_norm: str = "first",
-                 options: PlanOptions | None = None, group=None, hbm_budget: int | None = None):
+                 options: PlanOptions | None = None, group=None, hbm_budget: int | None = None,
+                 observed_first: int = 0):
         if grad_norm not in ("first", "none"):
             raise ValueError("grad_norm must be 'first' or 'none'")
         nx, nz = vel_init.shape
@@ -199,7 +191,7 @@ class Inversion:
                 raise ValueError("the plan-backed driver needs h, dt, w, sx, sy, ry and observed")
             local_fn = plan_residual_local_fn(nx, nz, h, dt, w, order, sx, sy, ry, observed,
                                               options=options, device=vel_init.device,
-                                              hbm_budget=hbm_budget)
+                                              hbm_budget=hbm_budget, observed_first=observed_first)
         self.model = PARAMETERS[parameter](vel_init.detach().clone(), vmin, vmax)
         self.optimizer = make_optimizer(self.model.parameters(), optimizer, lr, momentum)
         self.gradient_fn = ShardedGradient(local_fn, nshots, group=group)

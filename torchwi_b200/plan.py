@@ -70,6 +70,21 @@ def footprint_bytes(nx, nz, nt, nshots, order=4, wavelet_per_shot=False,
     return int(lay.workspace_bytes)
 
 
+def shot_blocks(shots: slice, nx, nz, nt, order=4, options: PlanOptions | None = None,
+                budget: int | None = None, device=None) -> list[slice]:
+    """Split `shots` into contiguous blocks whose plans each fit `budget`
+    bytes (default: 80 % of the device's free memory), halving the block size
+    until one fits; a single shot always makes a block."""
+    if budget is None:
+        free, _ = torch.cuda.mem_get_info(device)
+        budget = int(free * 0.8)
+    n = shots.stop - shots.start
+    per = max(n, 1)
+    while per > 1 and footprint_bytes(nx, nz, nt, per, order, options=options) > budget:
+        per = (per + 1) // 2
+    return [slice(a, min(a + per, shots.stop)) for a in range(shots.start, shots.stop, per)]
+
+
 def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions) -> Problem:
     if o.accumulate not in ("kahan", "plain"):
         raise ValueError("accumulate must be 'kahan' or 'plain'")
