@@ -34,6 +34,16 @@ MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjo
 TRAFFIC_SHOTS = 64                      # shots per launch of the captures in profiles/traffic.json
 
 
+def _launches_per_gradient(nt, K, time_block):
+    """Kernel launches of one gradient: model padding, the forward steps, the
+    two misfit passes, per checkpoint segment its recompute and adjoint
+    steps, the gradient reduction.  Two-step launches cover pairs of steps;
+    an odd remainder runs alone."""
+    per = (lambda n: (n + 1) // 2) if time_block == 2 else (lambda n: n)
+    segments = sum(per(min(K, nt - j * K)) for j in range((nt + K - 1) // K))
+    return 1 + per(nt) + 2 + 2 * segments + 1
+
+
 def _peak_hbm():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     try:
@@ -181,7 +191,12 @@ def run_b200(args):
     mine = slice(rank * NSHOTS, (rank + 1) * NSHOTS)
     sx, sy, ry = survey.sx[mine], survey.sy[mine], survey.ry[mine]
     opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
-                       shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True)
+                       shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True,
+                       time_block=args.time_block)
+    tuned_ms = None
+    if args.autotune:   # outside the timed region
+        from torchwi_b200 import autotune
+        opts, tuned_ms = autotune(NX, NZ, NSHOTS, 4, survey.h, survey.dt, opts, dev)
     plan = ShotPlan(NX, NZ, survey.h, survey.dt, NT, 4, nshots=NSHOTS, options=opts, device=dev)
     plan.set_wavelet(torch.from_numpy(survey.w))
     plan.set_shots(sx, sy, ry)
@@ -263,7 +278,7 @@ def run_b200(args):
     d2h = g_h.numel() * 4 + 8
 
     # per-kernel device time at steady state -> roofline of the dominant kernel
-    ms_launch = {m: plan.profile(m, repeats=args.profile_reps) for m in (0, 1, 2)}
+    ms_launch = {m: plan.profile_step(m, repeats=args.profile_reps) for m in (0, 1, 2)}
     dom = max(ms_launch, key=lambda m: ms_launch[m])
     cells = NSHOTS * NX * NZ
     achieved = ALG_BYTES[dom] * cells / (ms_launch[dom] / 1e3) / 1e9
@@ -313,8 +328,8 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
     if rank == 0:
-        # pad + forward nt + 2 misfit + recompute nt + adjoint nt + reduce
-        launches = args.steps * (3 * NT + 4)
+        launches = args.steps * _launches_per_gradient(NT, plan.layout.ckpt_interval,
+                                                       plan.layout.time_block)
         line = {
             "metric": "shot-gradients/s", "value": value, "unit": "shot-gradients/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -328,6 +343,8 @@ def run_b200(args):
                        "ckpt_interval": plan.layout.ckpt_interval,
                        "shots_per_cta": plan.layout.shots_per_cta,
                        "rows_per_warp": plan.layout.rows_per_warp,
+                       "time_block": plan.layout.time_block,
+                       "autotuned": bool(args.autotune),
                        "l2": "inputs larger than L2 (workspace %.1f GB)" % (plan.workspace.numel() / 1e9)},
             "gcell_per_s": gcell,
             "clocks": clocks,
@@ -340,7 +357,7 @@ def run_b200(args):
                          "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read+write per launch at "
                                            f"{TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}",
-                         "ms_per_launch": {MODE_NAMES[m]: v for m, v in ms_launch.items()}},
+                         "ms_per_time_step": {MODE_NAMES[m]: v for m, v in ms_launch.items()}},
             "plain_form": plain,
             "cpu_baseline": cpu,
         }
@@ -492,6 +509,8 @@ def main():
     ap.add_argument("--ckpt", type=int, default=0)
     ap.add_argument("--spc", type=int, default=0)
     ap.add_argument("--rz", type=int, default=0)
+    ap.add_argument("--time-block", type=int, default=0, help="time steps per launch (0 = plan default)")
+    ap.add_argument("--autotune", action="store_true", help="time the launch shapes first and use the fastest")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--profile-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")

@@ -136,6 +136,9 @@ typedef struct twi_problem {
     int exa;              /* 1: excitation-amplitude gradient (no checkpoints): the
                              forward pass keeps the largest virtual source per cell
                              and its step (16-bit, nt <= 32767); plan-level calls only */
+    int time_block;       /* time steps per launch of twi_forward / twi_gradient: 1, 2
+                             (the fields are read once per two steps), 0 = choose;
+                             excitation-amplitude plans always use 1 */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */
@@ -148,6 +151,7 @@ typedef struct twi_layout {
     size_t grad;            /* out: (nx, nz) float, z fastest (twi_gradient) */
     int dimx, dimz, pitch;  /* padded grid and its row pitch (floats) */
     int ckpt_interval, nsegments, shots_per_cta, rows_per_warp;
+    int time_block;         /* time steps per launch chosen for this plan */
 } twi_layout;
 
 typedef struct twi_plan twi_plan;
@@ -191,6 +195,21 @@ int twi_plan_check(twi_plan* plan, void* stream);
  * accumulators, never the checkpoints; call after twi_forward. */
 int twi_plan_profile(twi_plan* plan, int mode, int repeats, float* ms_per_launch, void* stream);
 int twi_plan_destroy(twi_plan* plan);
+/* Workspace bytes a plan of `prob` needs (host only; admission control). */
+int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes);
+
+/* Launch-shape autotuning (the reference has none: its CUDA path uses fixed
+ * 16x16 blocks, td2d_cuda.cu).  Times every launch shape that the fields of
+ * `prob` left at 0 allow -- shots per CTA 1/2/4/8 (at most nshots), rows per
+ * warp 4/8, one or two time steps per launch (one for excitation amplitude)
+ * -- on the current device, on a copy of the problem with nt = 8 in the
+ * caller's `scratch` (twi_autotune_scratch_bytes, any contents), and writes
+ * *prob with the fastest shape into `tuned` and, if not NULL, its device
+ * milliseconds per time step of a gradient (forward + recompute + adjoint;
+ * forward only for forward-only plans).  Synchronises `stream`. */
+int twi_autotune_scratch_bytes(const twi_problem* prob, size_t* bytes);
+int twi_autotune(const twi_problem* prob, void* scratch, size_t scratch_bytes, void* stream,
+                 twi_problem* tuned, float* ms_per_step);
 
 /* ------------------------------------------------------------------------
  * 3. Batches of plans

@@ -124,3 +124,38 @@ def test_exa_plan_ignores_kahan():
         L.twi_plan_destroy(h)
         sizes.append(lay.workspace_bytes)
     assert sizes[0] == sizes[1]
+
+
+def test_footprint_and_autotune_scratch_on_host():
+    L = _capi.lib()
+    n = ctypes.c_size_t()
+    p = _problem(nt=300, nshots=8, nx=70, nz=33)
+    assert L.twi_plan_footprint_bytes(ctypes.byref(p), ctypes.byref(n)) == 0
+    st, h = _create(nt=300, nshots=8, nx=70, nz=33)
+    lay = _capi.Layout()
+    L.twi_plan_layout(h, ctypes.byref(lay))
+    L.twi_plan_destroy(h)
+    assert n.value == lay.workspace_bytes
+    m = ctypes.c_size_t()
+    assert L.twi_autotune_scratch_bytes(ctypes.byref(p), ctypes.byref(m)) == 0
+    assert 0 < m.value < n.value            # short copies of the problem
+    bad = _problem(order=6)
+    assert L.twi_autotune_scratch_bytes(ctypes.byref(bad), ctypes.byref(m)) == _capi.TWI_ERR_INVALID
+
+
+def test_time_block_option_on_host():
+    L = _capi.lib()
+    for tb, want in ((0, 1), (1, 1), (2, 2)):
+        st, h = _create(nt=100, nshots=2, time_block=tb)
+        assert st == 0
+        lay = _capi.Layout()
+        L.twi_plan_layout(h, ctypes.byref(lay))
+        L.twi_plan_destroy(h)
+        assert lay.time_block == want
+    st, h = _create(time_block=3)
+    assert st == _capi.TWI_ERR_INVALID
+    st, h = _create(nt=100, nshots=2, time_block=2, exa=1)   # excitation amplitude: one step
+    lay = _capi.Layout()
+    L.twi_plan_layout(h, ctypes.byref(lay))
+    L.twi_plan_destroy(h)
+    assert lay.time_block == 1

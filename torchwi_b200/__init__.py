@@ -5,6 +5,9 @@ Public API (mirrors torchwi.operator / torchwi.propagator):
     Time2d, Time2dForward        reference-compatible modules
     Time2dBatch                  all shots of a survey in one plan
     ShotPlan, PlanOptions        the underlying C-ABI plan
+    autotune                     fastest launch shape for a grid and shot count
+    inversion.Inversion          FWI driver over the batched plan
+    io, workflows                RSF / gather files and the example programs
     propagator.td2d_b200         drop-in for the native td2d_cuda module
     source.ricker, source.fdgaus input wavelets
 
@@ -13,7 +16,7 @@ build it with ``python -m torchwi_b200.build``.
 """
 
 from .operator import Time2d, Time2dBatch, Time2dForward  # noqa: F401
-from .plan import PlanBatch, PlanOptions, ShotPlan, footprint_bytes  # noqa: F401
+from .plan import PlanBatch, PlanOptions, ShotPlan, autotune, footprint_bytes  # noqa: F401
 from .source import fdgaus, ricker  # noqa: F401
 from ._capi import TwiError, TwiInvalid  # noqa: F401
 

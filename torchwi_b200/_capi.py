@@ -37,7 +37,8 @@ class Problem(ctypes.Structure):
                 ("exact", ctypes.c_int), ("accumulate", ctypes.c_int),
                 ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int),
                 ("use_graphs", ctypes.c_int), ("wavelet_per_shot", ctypes.c_int),
-                ("forward_only", ctypes.c_int), ("exa", ctypes.c_int)]
+                ("forward_only", ctypes.c_int), ("exa", ctypes.c_int),
+                ("time_block", ctypes.c_int)]
 
 
 class Layout(ctypes.Structure):
@@ -46,7 +47,8 @@ class Layout(ctypes.Structure):
                 ("resid", ctypes.c_size_t), ("grad", ctypes.c_size_t),
                 ("dimx", ctypes.c_int), ("dimz", ctypes.c_int), ("pitch", ctypes.c_int),
                 ("ckpt_interval", ctypes.c_int), ("nsegments", ctypes.c_int),
-                ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int)]
+                ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int),
+                ("time_block", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p
@@ -74,6 +76,9 @@ SIGNATURES = {
     "twi_plan_check": [_vp, _vp],
     "twi_plan_profile": [_vp, _i, _i, ctypes.POINTER(ctypes.c_float), _vp],
     "twi_plan_destroy": [_vp],
+    "twi_plan_footprint_bytes": [_vp, ctypes.POINTER(ctypes.c_size_t)],
+    "twi_autotune_scratch_bytes": [_vp, ctypes.POINTER(ctypes.c_size_t)],
+    "twi_autotune": [_vp, _vp, ctypes.c_size_t, _vp, _vp, ctypes.POINTER(ctypes.c_float)],
     "twi_batch_create": [ctypes.POINTER(_vp), _i, ctypes.POINTER(_vp)],
     "twi_batch_workspace_size": [_vp, ctypes.POINTER(ctypes.c_size_t)],
     "twi_batch_bind": [_vp, _vp, ctypes.c_size_t],

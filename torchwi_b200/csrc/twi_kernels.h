@@ -38,6 +38,7 @@ struct StepArgs {
     int prev_base, prev_stride;
     int cur_base, cur_stride;
     int next_base, next_stride;
+    int next2_base, next2_stride;   // second output of a two-step launch (twi_step2.cu)
     int nshots;   // shots in this launch (grid.z * spc covers them)
     int spc;      // shots per CTA
     int it;       // time index of this step
@@ -147,6 +148,20 @@ __host__ __device__ constexpr int zhalo(int order) { return order / 2; }
 // and this many cells per thread, ahead of the interior tiles in the grid.
 constexpr int kBoundaryCellsPerThread = 4;
 constexpr int kThreads = 128;
+
+// Two-step launches (twi_step2.cu): output tiles of kTile2X columns.  tm_un
+// is a tensor map over the field slots with a (136, 4*rows_per_warp + 2*order)
+// box, tm_um the same slots with a (128, 4*rows_per_warp + order) box and
+// tm_v the padded velocity with that box (step2_box_rows gives the rows:
+// which = 0 for tm_un, 1 for the others).  Modes 0-2; step A is time a.it,
+// step B a.it + 1 (a.it - 1 for the adjoint).
+constexpr int kTile2X = 120;
+long long step2_ctas(int order, int rows_per_warp, const StepArgs& a);
+int step2_box_rows(int order, int rows_per_warp, int which);
+cudaError_t launch_step2(int order, bool exact, StepMode mode, LaunchShape shape,
+                         const CUtensorMap& tm_un, const CUtensorMap& tm_um, const CUtensorMap& tm_v,
+                         const StepArgs& a, cudaStream_t stream);
+cudaError_t prepare_step2(int order, bool exact, LaunchShape shape);
 
 // Store n host integers into device memory through kernel parameters
 // (chunks of 2048), ordered on `stream` without a host synchronisation.

@@ -8,10 +8,11 @@
 // (no copies) and the recompute/adjoint passes read them back in place.
 //
 // Slot map of one shot (SPS slots per shot, global slot 0 is all zeros and
-// stands for u^{-1} = u^0 = lambda^{-1} = lambda^{-2} = 0):
-//   1 + s*SPS + {0,1,2}          forward/recompute rotation  u^k, k mod 3
-//   1 + s*SPS + {3,4,5}          adjoint rotation            lambda
-//   1 + s*SPS + 6 + 2(j-1) + p   checkpoint j >= 1: p=0 -> u^{jK-1}, p=1 -> u^{jK}
+// stands for u^{-1} = u^0 = lambda^{-1} = lambda^{-2} = 0; ROT = 3, or 4 when
+// two time steps run per launch so that both outputs avoid both inputs):
+//   1 + s*SPS + [0, ROT)                forward/recompute rotation  u^k, k mod ROT
+//   1 + s*SPS + ROT + [0, ROT)          adjoint rotation            lambda
+//   1 + s*SPS + 2ROT + 2(j-1) + p       checkpoint j >= 1: p=0 -> u^{jK-1}, p=1 -> u^{jK}
 // Gradient pass, segment j = nseg-1 .. 0 (K steps each, the last may be
 // shorter): recompute u^{jK+1..jK+L} from checkpoint j writing the virtual
 // source of each step into a K-slot buffer per shot, then run the L adjoint
@@ -137,6 +138,9 @@ int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, in
     return TWI_OK;
 }
 
+// Time steps per launch when the problem leaves it open.
+constexpr int kDefaultTimeBlock = 1;
+
 LaunchShape default_shape(int rows_per_warp) {
     return LaunchShape{rows_per_warp == 8 ? 8 : 4, 4};
 }
@@ -152,6 +156,7 @@ struct twi_plan {
     int ne = 0, dimx = 0, dimz = 0, pitch = 0;
     long long slot_elems = 0;
     int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
+    int tb = 1, rot = 3;   // time steps per launch (1 or 2) and rotation slots per role
     bool gradient = true, kahan = true, exa = false;
     long long nslots = 0, nvirt = 0, nacc = 0;
     // workspace regions (byte offsets)
@@ -161,6 +166,7 @@ struct twi_plan {
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
+    CUtensorMap tm2_un{}, tm2_um{}, tm2_v{};   // two-step launches
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
     cudaGraphExec_t g_bwd = nullptr;
@@ -184,8 +190,8 @@ struct twi_plan {
 
     Slot zero() const { return {0, 0}; }
     Slot urot(int i) const { return {1 + i, sps}; }
-    Slot lrot(int i) const { return {4 + i, sps}; }
-    Slot ckpt(int j, int part) const { return {1 + 6 + 2 * (j - 1) + part, sps}; }
+    Slot lrot(int i) const { return {1 + rot + i, sps}; }
+    Slot ckpt(int j, int part) const { return {1 + 2 * rot + 2 * (j - 1) + part, sps}; }
 
     // slot of u^k during the forward pass
     Slot fwd_slot(long long k, bool save) const {
@@ -194,15 +200,15 @@ struct twi_plan {
             if (k % K == 0 && k / K < nseg) return ckpt((int)(k / K), 1);
             if ((k + 1) % K == 0 && (k + 1) / K < nseg) return ckpt((int)((k + 1) / K), 0);
         }
-        return urot((int)(k % 3));
+        return urot((int)(k % rot));
     }
     // slot of u^k while recomputing segment j
     Slot rec_slot(long long k, int j) const {
         const long long c = (long long)j * K;
         if (k <= c) return j == 0 ? zero() : ckpt(j, k == c ? 1 : 0);
-        return urot((int)(k % 3));
+        return urot((int)(k % rot));
     }
-    Slot lam_slot(long long m) const { return m < 0 ? zero() : lrot((int)(m % 3)); }
+    Slot lam_slot(long long m) const { return m < 0 ? zero() : lrot((int)(m % rot)); }
 
     StepArgs base_args() const {
         StepArgs a{};
@@ -235,9 +241,10 @@ struct twi_plan {
         return a;
     }
 
-    int launch(StepMode mode, const StepArgs& a, cudaStream_t st) const {
-        cudaError_t e = launch_step(p.order, p.exact != 0, mode, default_shape(rz), tm_u2, tm_u1,
-                                    tm_vel, a, st);
+    int launch(StepMode mode, const StepArgs& a, cudaStream_t st, int nsteps = 1) const {
+        cudaError_t e = nsteps == 2
+            ? launch_step2(p.order, p.exact != 0, mode, default_shape(rz), tm2_un, tm2_um, tm2_v, a, st)
+            : launch_step(p.order, p.exact != 0, mode, default_shape(rz), tm_u2, tm_u1, tm_vel, a, st);
         if (e != cudaSuccess)
             return fail(TWI_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
         return TWI_OK;
@@ -245,23 +252,31 @@ struct twi_plan {
 
     using Step = TwiStep;
 
-    // The forward pass as a list of time steps.
-    void forward_steps(bool save, std::vector<Step>& out) const {
+    static void set_slots(StepArgs& a, Slot pv, Slot cu, Slot nx, Slot nx2) {
+        a.prev_base = pv.base, a.prev_stride = pv.stride;
+        a.cur_base = cu.base, a.cur_stride = cu.stride;
+        a.next_base = nx.base, a.next_stride = nx.stride;
+        a.next2_base = nx2.base, a.next2_stride = nx2.stride;
+    }
+
+    // The forward pass as a list of launches: pairs of time steps when the
+    // plan runs two per launch (`blocked`), else single steps.
+    void forward_steps(bool save, std::vector<Step>& out, bool blocked) const {
         StepArgs a = base_args();
         a.frd = F(off_frd);
         const StepMode mode = save && exa ? kModeExaForward : kModeForward;
         if (exa) {
             a.exa = F(off_exa);
             a.iexa = reinterpret_cast<short*>(ws + off_iexa);
+            blocked = false;
         }
-        for (int it = 0; it < p.nt; ++it) {
-            const Slot pv = fwd_slot(it - 1, save), cu = fwd_slot(it, save),
-                       nx_ = fwd_slot(it + 1, save);
+        for (int it = 0; it < p.nt;) {
+            const int n = blocked && it + 1 < p.nt ? 2 : 1;
             a.it = it;
-            a.prev_base = pv.base, a.prev_stride = pv.stride;
-            a.cur_base = cu.base, a.cur_stride = cu.stride;
-            a.next_base = nx_.base, a.next_stride = nx_.stride;
-            out.push_back({mode, a});
+            set_slots(a, fwd_slot(it - 1, save), fwd_slot(it, save), fwd_slot(it + 1, save),
+                      n == 2 ? fwd_slot(it + 2, save) : zero());
+            out.push_back({mode, a, n});
+            it += n;
         }
     }
 
@@ -286,8 +301,8 @@ struct twi_plan {
     }
 
     // The gradient pass (without the accumulator reset and the final
-    // reduction) as a list of time steps: per segment, recompute then adjoint.
-    void gradient_steps(std::vector<Step>& out) const {
+    // reduction) as a list of launches: per segment, recompute then adjoint.
+    void gradient_steps(std::vector<Step>& out, bool blocked) const {
         if (exa) return exa_gradient_steps(out);
         StepArgs a = base_args();
         a.virt_out = F(off_virt);
@@ -301,25 +316,25 @@ struct twi_plan {
         for (int j = nseg - 1; j >= 0; --j) {
             const int c0 = j * K;
             const int L = std::min(K, p.nt - c0);
-            for (int it = c0; it < c0 + L; ++it) {     // recompute, writing virt
-                const Slot pv = rec_slot(it - 1, j), cu = rec_slot(it, j), nx_ = urot((it + 1) % 3);
+            for (int it = c0; it < c0 + L;) {     // recompute, writing virt
+                const int n = blocked && it + 1 < c0 + L ? 2 : 1;
                 a.it = it;
-                a.prev_base = pv.base, a.prev_stride = pv.stride;
-                a.cur_base = cu.base, a.cur_stride = cu.stride;
-                a.next_base = nx_.base, a.next_stride = nx_.stride;
+                set_slots(a, rec_slot(it - 1, j), rec_slot(it, j), urot((it + 1) % rot),
+                          n == 2 ? urot((it + 2) % rot) : zero());
                 a.virt_base = it - c0;
                 a.frd = nullptr;
-                out.push_back({kModeRecompute, a});
+                out.push_back({kModeRecompute, a, n});
+                it += n;
             }
-            for (int it = c0 + L - 1; it >= c0; --it) {  // adjoint, reading virt
+            for (int it = c0 + L - 1; it >= c0;) {  // adjoint, reading virt
+                const int n = blocked && it - 1 >= c0 ? 2 : 1;
                 const long long m = (long long)p.nt - 1 - it;
-                const Slot pv = lam_slot(m - 2), cu = lam_slot(m - 1), nx_ = lam_slot(m);
                 a.it = it;
-                a.prev_base = pv.base, a.prev_stride = pv.stride;
-                a.cur_base = cu.base, a.cur_stride = cu.stride;
-                a.next_base = nx_.base, a.next_stride = nx_.stride;
+                set_slots(a, lam_slot(m - 2), lam_slot(m - 1), lam_slot(m),
+                          n == 2 ? lam_slot(m + 1) : zero());
                 a.virt_base = it - c0;
-                out.push_back({kModeAdjoint, a});
+                out.push_back({kModeAdjoint, a, n});
+                it -= n;
             }
         }
     }
@@ -349,10 +364,10 @@ struct twi_plan {
             TWI_CUDA(cudaMemsetAsync(ws + off_iexa, 0, (size_t)p.nshots * slot_elems * 2, st));
         }
         std::vector<Step> steps;
-        forward_steps(save, steps);
+        forward_steps(save, steps, tb == 2);
         for (Step& s : steps) {
             s.a.obs = obs;
-            TWI_TRY(launch(s.mode, s.a, st));
+            TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
         }
         if (misfit) {
             cudaError_t e = launch_misfit(F(off_frd), (long long)p.nshots * p.nt * p.nx,
@@ -365,8 +380,8 @@ struct twi_plan {
     int enqueue_gradient(cudaStream_t st) const {
         TWI_TRY(gradient_prologue(st));
         std::vector<Step> steps;
-        gradient_steps(steps);
-        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st));
+        gradient_steps(steps, tb == 2);
+        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
         return gradient_epilogue(st);
     }
 
@@ -447,7 +462,13 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     if (spc <= 0) spc = std::min(p.nshots, 4);
     P->spc = std::min(spc, p.nshots);
     P->ngroups = (p.nshots + P->spc - 1) / P->spc;
-    P->sps = P->exa ? 6 : P->gradient ? 6 + 2 * (P->nseg - 1) : 3;
+    if (p.time_block < 0 || p.time_block > 2) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "time_block must be 0 (choose), 1 or 2");
+    }
+    P->tb = P->exa ? 1 : p.time_block == 0 ? kDefaultTimeBlock : p.time_block;
+    P->rot = P->tb == 2 ? 4 : 3;
+    P->sps = P->gradient ? 2 * P->rot + (P->exa ? 0 : 2 * (P->nseg - 1)) : P->rot;
     P->nslots = 1 + (long long)p.nshots * P->sps;
     P->nvirt = P->gradient && !P->exa ? (long long)p.nshots * K : 0;
     P->nacc = P->gradient ? (P->kahan ? P->ngroups : p.nshots) : 0;
@@ -487,6 +508,7 @@ int twi_plan_layout(const twi_plan* P, twi_layout* out) {
     out->dimz = P->dimz;
     out->pitch = P->pitch;
     out->ckpt_interval = P->K;
+    out->time_block = P->tb;
     out->nsegments = P->nseg;
     out->shots_per_cta = P->spc;
     out->rows_per_warp = P->rz;
@@ -510,6 +532,15 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
     TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
                      TZ));
     TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
+    if (P->tb == 2) {
+        TWI_CUDA(prepare_step2(P->p.order, P->p.exact != 0, default_shape(P->rz)));
+        const int rn = step2_box_rows(P->p.order, P->rz, 0), ra = step2_box_rows(P->p.order, P->rz, 1);
+        TWI_TRY(make_map(&P->tm2_un, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch,
+                         kTileX + 8, rn));
+        TWI_TRY(make_map(&P->tm2_um, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch,
+                         kTileX, ra));
+        TWI_TRY(make_map(&P->tm2_v, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, ra));
+    }
     // the zero slot, error word and velocity padding columns are cleared on
     // the caller's stream by the next set_shots / set_model
     P->need_zero = true;
@@ -609,8 +640,11 @@ int twi_plan_check(twi_plan* P, void* stream) {
 
 int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, void* stream) {
     if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    const int nsteps = mode >= 10 ? 2 : 1;
+    mode = mode >= 10 ? mode - 10 : mode;
     if (!ms_per_launch || repeats < 1 || mode < 0 || mode > 2)
-        return fail(TWI_ERR_INVALID, "mode must be 0, 1 or 2 and repeats >= 1");
+        return fail(TWI_ERR_INVALID, "mode must be 0, 1, 2 (one step) or 10, 11, 12 (two steps) and repeats >= 1");
+    if (nsteps == 2 && P->tb != 2) return fail(TWI_ERR_INVALID, "two-step launches need a plan with time_block 2");
     if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     StepArgs a = P->base_args();
@@ -618,25 +652,27 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
     a.it = it;
     const StepMode m = static_cast<StepMode>(mode);
     if (m == kModeAdjoint) {
-        a.prev_base = 4, a.cur_base = 5, a.next_base = 6;   // adjoint rotation
+        const Slot l0 = P->lrot(0), l1 = P->lrot(1), l2 = P->lrot(2), l3 = P->lrot(P->rot - 1);
+        a.prev_base = l0.base, a.cur_base = l1.base, a.next_base = l2.base, a.next2_base = l3.base;
         a.virt_in = P->F(P->off_virt);
         a.resid = P->F(P->off_frd);
         a.acc = P->F(P->off_acc);
         a.acc_comp = P->kahan ? P->F(P->off_comp) : nullptr;
         a.acc_mode = P->kahan ? kAccKahanPerGroup : kAccPlainPerShot;
     } else {
-        a.prev_base = 1, a.cur_base = 2, a.next_base = 3;   // forward rotation
+        const Slot u0 = P->urot(0), u1 = P->urot(1), u2 = P->urot(2), u3 = P->urot(P->rot - 1);
+        a.prev_base = u0.base, a.cur_base = u1.base, a.next_base = u2.base, a.next2_base = u3.base;
         if (m == kModeRecompute) a.virt_out = P->F(P->off_virt);
     }
-    a.prev_stride = a.cur_stride = a.next_stride = P->sps;
+    a.prev_stride = a.cur_stride = a.next_stride = a.next2_stride = P->sps;
     a.virt_stride = P->K;
-    a.virt_base = 0;
+    a.virt_base = m == kModeAdjoint ? 1 : 0;   // two-step adjoint reads slots 1 and 0
     cudaEvent_t e0, e1;
     TWI_CUDA(cudaEventCreate(&e0));
     TWI_CUDA(cudaEventCreate(&e1));
     int s = TWI_OK;
     if (cudaEventRecord(e0, st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event record failed");
-    for (int r = 0; r < repeats && s == TWI_OK; ++r) s = P->launch(m, a, st);
+    for (int r = 0; r < repeats && s == TWI_OK; ++r) s = P->launch(m, a, st, nsteps);
     if (s == TWI_OK && cudaEventRecord(e1, st) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event record failed");
     if (s == TWI_OK && cudaEventSynchronize(e1) != cudaSuccess) s = fail(TWI_ERR_CUDA, "event sync failed");
     float ms = 0.f;
@@ -645,6 +681,104 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
     cudaEventDestroy(e1);
     if (s == TWI_OK) *ms_per_launch = ms / repeats;
     return s;
+}
+
+int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes) {
+    if (!prob || !bytes) return fail(TWI_ERR_INVALID, "null argument");
+    twi_plan* P = nullptr;
+    TWI_TRY(twi_plan_create(prob, &P));
+    *bytes = P->total;
+    delete P;
+    return TWI_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The launch shapes the autotuner tries for `prob`: every combination the
+// caller left open (0) of shots per CTA {1, 2, 4, 8} (at most nshots), rows
+// per warp {4, 8} and time steps per launch {1, 2} (1 for excitation
+// amplitude), each timed on a copy of the problem with nt = 8.
+std::vector<twi_problem> tune_candidates(const twi_problem& p) {
+    std::vector<twi_problem> out;
+    for (int spc : {1, 2, 4, 8}) {
+        if (p.shots_per_cta ? spc != p.shots_per_cta : spc > std::max(1, p.nshots)) continue;
+        for (int rz : {4, 8}) {
+            if (p.rows_per_warp && rz != p.rows_per_warp) continue;
+            for (int tb : {1, 2}) {
+                if ((p.time_block && tb != p.time_block) || (p.exa && tb == 2)) continue;
+                twi_problem q = p;
+                q.nt = 8;
+                q.ckpt_interval = 2;
+                q.use_graphs = 0;
+                q.shots_per_cta = spc, q.rows_per_warp = rz, q.time_block = tb;
+                out.push_back(q);
+            }
+        }
+    }
+    return out;
+}
+
+}  // namespace
+
+extern "C" {
+
+int twi_autotune_scratch_bytes(const twi_problem* prob, size_t* bytes) {
+    if (!prob || !bytes) return fail(TWI_ERR_INVALID, "null argument");
+    size_t most = 0;
+    for (const twi_problem& q : tune_candidates(*prob)) {
+        size_t b = 0;
+        TWI_TRY(twi_plan_footprint_bytes(&q, &b));
+        most = std::max(most, b);
+    }
+    if (most == 0) return fail(TWI_ERR_INVALID, "no launch shape fits the fixed fields of the problem");
+    *bytes = most;
+    return TWI_OK;
+}
+
+int twi_autotune(const twi_problem* prob, void* scratch, size_t scratch_bytes, void* stream,
+                 twi_problem* tuned, float* ms_per_step) {
+    if (!prob || !scratch || !tuned) return fail(TWI_ERR_INVALID, "null argument");
+    const std::vector<twi_problem> cands = tune_candidates(*prob);
+    if (cands.empty()) return fail(TWI_ERR_INVALID, "no launch shape fits the fixed fields of the problem");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // shots in the middle of the model, receivers two cells down
+    const int S = prob->nshots;
+    std::vector<float> sx(S, prob->h * (prob->nx / 2)), sy(S, prob->h * std::min(2, prob->nz - 1));
+    const std::vector<float> vel((size_t)prob->nx * prob->nz, 2000.f);   // a uniform model
+    float best = -1.f;
+    twi_problem best_q{};
+    for (const twi_problem& q : cands) {
+        twi_plan* P = nullptr;
+        TWI_TRY(twi_plan_create(&q, &P));
+        int s = twi_plan_bind(P, scratch, scratch_bytes);
+        if (s == TWI_OK && cudaMemsetAsync(scratch, 0, P->total, st) != cudaSuccess)
+            s = fail(TWI_ERR_CUDA, "scratch clear failed");
+        if (s == TWI_OK) s = twi_plan_set_shots(P, sx.data(), sy.data(), sy.data(), stream);
+        if (s == TWI_OK && cudaMemcpyAsync(P->F(P->off_vel), vel.data(), vel.size() * 4,
+                                           cudaMemcpyHostToDevice, st) != cudaSuccess)
+            s = fail(TWI_ERR_CUDA, "model upload failed");
+        if (s == TWI_OK) s = twi_plan_set_model(P, stream);
+        float total = 0.f;
+        const int modes = P->gradient ? 3 : 1;
+        for (int m = 0; m < modes && s == TWI_OK; ++m) {
+            const int mode = P->tb == 2 ? 10 + m : m;
+            float ms = 0.f;
+            s = twi_plan_profile(P, mode, 2, &ms, stream);           // warm-up
+            if (s == TWI_OK) s = twi_plan_profile(P, mode, 10, &ms, stream);
+            total += ms / P->tb;
+        }
+        twi_plan_destroy(P);
+        if (s != TWI_OK) return s;
+        if (best < 0.f || total < best) best = total, best_q = q;
+    }
+    *tuned = *prob;
+    tuned->shots_per_cta = best_q.shots_per_cta;
+    tuned->rows_per_warp = best_q.rows_per_warp;
+    tuned->time_block = best_q.time_block;
+    if (ms_per_step) *ms_per_step = best;
+    return TWI_OK;
 }
 
 int twi_plan_destroy(twi_plan* P) {
@@ -671,9 +805,9 @@ long long plan_gathers_elems(const twi_plan* P) {
     return (long long)P->p.nshots * P->p.nt * P->p.nx;
 }
 void plan_steps(const twi_plan* P, int kind, std::vector<TwiStep>& out, size_t* fwd_steps) {
-    P->forward_steps(kind == 1, out);
+    P->forward_steps(kind == 1, out, false);
     *fwd_steps = out.size();
-    if (kind == 1) P->gradient_steps(out);
+    if (kind == 1) P->gradient_steps(out, false);
 }
 int plan_gradient_prologue(const twi_plan* P, cudaStream_t st) { return P->gradient_prologue(st); }
 int plan_gradient_epilogue(const twi_plan* P, cudaStream_t st) { return P->gradient_epilogue(st); }
@@ -722,8 +856,8 @@ struct twi_batch {
     void steps_of(int phase, std::vector<std::vector<twi_plan::Step>>& per) const {
         per.assign(plans.size(), {});
         for (size_t i = 0; i < plans.size(); ++i) {
-            if (phase == 2) plans[i]->gradient_steps(per[i]);
-            else plans[i]->forward_steps(phase == 1, per[i]);
+            if (phase == 2) plans[i]->gradient_steps(per[i], false);
+            else plans[i]->forward_steps(phase == 1, per[i], false);
         }
     }
 

@@ -9,10 +9,13 @@
 
 namespace twi {
 
-// One time step of one plan: the kernel mode and its arguments.
+// One launch of one plan: the kernel mode, its arguments and the time steps
+// it advances (1, or 2 for the two-step kernel; the engine and batches use
+// single steps only).
 struct TwiStep {
     StepMode mode;
     StepArgs a;
+    int nsteps = 1;
 };
 
 }  // namespace twi

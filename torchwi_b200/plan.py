@@ -38,6 +38,9 @@ class PlanOptions:
                  no checkpoints; the forward pass keeps the largest virtual
                  source per cell and its step, the adjoint assigns
                  -exa*lambda at that step.  nt <= 32767.
+    time_block:  time steps per kernel launch in forward and gradient passes
+                 (1 or 2; 0 = the library's choice).  Two steps read the
+                 wavefields once per two steps; results are identical.
     """
 
     exact: bool = True
@@ -48,6 +51,7 @@ class PlanOptions:
     use_graphs: bool = True
     forward_only: bool = False
     exa: bool = False
+    time_block: int = 0
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -59,15 +63,44 @@ def footprint_bytes(nx, nz, nt, nshots, order=4, wavelet_per_shot=False,
     """Workspace bytes a plan of this size needs (for HBM admission)."""
     o = options or PlanOptions()
     prob = _problem(nx, nz, nt, 10.0, 1e-3, nshots, order, wavelet_per_shot, o)
+    n = ctypes.c_size_t()
+    check(_capi.lib().twi_plan_footprint_bytes(ctypes.byref(prob), ctypes.byref(n)))
+    return int(n.value)
+
+
+_TUNED: dict = {}
+
+
+def autotune(nx, nz, nshots, order=4, h=10.0, dt=1e-3, options: PlanOptions | None = None,
+             device=None) -> tuple[PlanOptions, float]:
+    """Fastest launch shape (shots per CTA, rows per warp, time steps per
+    launch) for plans of this grid and shot count on `device`, timed by the
+    library on a short copy of the problem; fields already set (non-zero) in
+    `options` stay fixed.  Returns (options with the shape filled in, device
+    milliseconds per time step of a gradient).  Results are cached per
+    problem and device."""
+    o = options or PlanOptions()
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    key = (dev.index, nx, nz, nshots, order, o.exact, o.accumulate, o.forward_only, o.exa,
+           o.shots_per_cta, o.rows_per_warp, o.time_block)
+    if key in _TUNED:
+        return _TUNED[key]
+    import dataclasses
+    prob = _problem(nx, nz, 8, h, dt, nshots, order, False, o)
     L = _capi.lib()
-    h = ctypes.c_void_p()
-    check(L.twi_plan_create(ctypes.byref(prob), ctypes.byref(h)))
-    lay = Layout()
-    try:
-        check(L.twi_plan_layout(h, ctypes.byref(lay)))
-    finally:
-        L.twi_plan_destroy(h)
-    return int(lay.workspace_bytes)
+    n = ctypes.c_size_t()
+    check(L.twi_autotune_scratch_bytes(ctypes.byref(prob), ctypes.byref(n)))
+    with torch.cuda.device(dev):
+        scratch = torch.empty(int(n.value), dtype=torch.uint8, device=dev)
+        tuned = Problem()
+        ms = ctypes.c_float()
+        check(L.twi_autotune(ctypes.byref(prob), ctypes.c_void_p(scratch.data_ptr()), n,
+                             _stream_handle(), ctypes.byref(tuned), ctypes.byref(ms)))
+    res = (dataclasses.replace(o, shots_per_cta=int(tuned.shots_per_cta),
+                               rows_per_warp=int(tuned.rows_per_warp),
+                               time_block=int(tuned.time_block)), float(ms.value))
+    _TUNED[key] = res
+    return res
 
 
 def shot_blocks(shots: slice, nx, nz, nt, order=4, options: PlanOptions | None = None,
@@ -93,7 +126,8 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    accumulate=0 if o.accumulate == "kahan" else 1,
                    shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
                    use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
-                   forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)))
+                   forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)),
+                   time_block=int(o.time_block))
 
 
 class ShotPlan:
@@ -201,9 +235,18 @@ class ShotPlan:
             check(self._lib.twi_gradient(self._h, _stream_handle()))
         return self.grad
 
+    def profile_step(self, mode: int, repeats: int = 20) -> float:
+        """Mean device milliseconds per TIME STEP of one kernel mode (0
+        forward, 1 recompute, 2 adjoint) as this plan launches it: a two-step
+        launch's time is halved."""
+        if self.layout.time_block == 2:
+            return self.profile(10 + mode, repeats) / 2
+        return self.profile(mode, repeats)
+
     def profile(self, mode: int, repeats: int = 20) -> float:
         """Mean device milliseconds per launch of one kernel mode (0 forward,
-        1 recompute, 2 adjoint) at steady state, all shots."""
+        1 recompute, 2 adjoint; 10, 11, 12 the two-step launches of a plan
+        with time_block 2) at steady state, all shots."""
         ms = ctypes.c_float()
         with torch.cuda.device(self.device):
             check(self._lib.twi_plan_profile(self._h, int(mode), int(repeats), ctypes.byref(ms),
