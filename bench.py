@@ -192,7 +192,7 @@ def run_b200(args):
     sx, sy, ry = survey.sx[mine], survey.sy[mine], survey.ry[mine]
     opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
                        shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True,
-                       time_block=args.time_block)
+                       time_block=args.time_block, reconstruct=args.reconstruct)
     tuned_ms = None
     if args.autotune:   # outside the timed region
         from torchwi_b200 import autotune
@@ -283,6 +283,10 @@ def run_b200(args):
     cells = NSHOTS * NX * NZ
     achieved = ALG_BYTES[dom] * cells / (ms_launch[dom] / 1e3) / 1e9
     peak, peak_kind = _peak_hbm()
+    # a reconstruction plan's second pass rebuilds the field backwards
+    names = dict(MODE_NAMES)
+    if args.reconstruct:
+        names[1] = "reverse reconstruction step (+virtual source)"
     # DRAM bytes per launch from one ncu capture of each mode at 64 shots on
     # this grid; a launch's traffic grows with the shots it processes, so
     # other shot counts scale it by NSHOTS / 64
@@ -345,19 +349,21 @@ def run_b200(args):
                        "rows_per_warp": plan.layout.rows_per_warp,
                        "time_block": plan.layout.time_block,
                        "autotuned": bool(args.autotune),
+                       "adjoint_wavefield": "boundary saving, reverse reconstruction" if args.reconstruct
+                                            else f"checkpoints every {plan.layout.ckpt_interval} steps",
                        "l2": "inputs larger than L2 (workspace %.1f GB)" % (plan.workspace.numel() / 1e9)},
             "gcell_per_s": gcell,
             "clocks": clocks,
             "e2e": {"value": total_shots / (ms_e2e / 1e3), "unit": "shot-gradients/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": MODE_NAMES[dom], "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
                          "traffic_source": "ncu dram__bytes_read+write per launch at "
                                            f"{TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}",
-                         "ms_per_time_step": {MODE_NAMES[m]: v for m, v in ms_launch.items()}},
+                         "ms_per_time_step": {names[m]: v for m, v in ms_launch.items()}},
             "plain_form": plain,
             "cpu_baseline": cpu,
         }
@@ -511,6 +517,8 @@ def main():
     ap.add_argument("--rz", type=int, default=0)
     ap.add_argument("--time-block", type=int, default=0, help="time steps per launch (0 = plan default)")
     ap.add_argument("--autotune", action="store_true", help="time the launch shapes first and use the fastest")
+    ap.add_argument("--reconstruct", action="store_true",
+                    help="boundary saving + reverse reconstruction instead of checkpoints")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--profile-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")

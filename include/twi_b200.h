@@ -139,6 +139,14 @@ typedef struct twi_problem {
     int time_block;       /* time steps per launch of twi_forward / twi_gradient: 1, 2
                              (the fields are read once per two steps), 0 = choose;
                              excitation-amplitude plans always use 1 */
+    int reconstruct;      /* 1: boundary saving instead of checkpoints -- the forward
+                             pass keeps the Keys cells of every time level, the
+                             gradient pass rebuilds the wavefield backwards from the
+                             last two levels; (nt+1) * nshots * boundary cells floats
+                             instead of the checkpoint and virtual-source slots.
+                             Gradients agree with the reference within its FP32
+                             tolerance, not bit for bit.  One step per launch;
+                             plan-level calls only */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */
@@ -189,9 +197,11 @@ int twi_gradient(twi_plan* plan, void* stream);
 int twi_plan_check(twi_plan* plan, void* stream);
 /* Measurement hook (no counterpart in the reference): launch `repeats`
  * steady-state time steps of one kernel mode (0 forward, 1 recompute with
- * virtual-source output, 2 adjoint with gradient accumulation) for all shots
- * and return the mean device time per launch in *ms_per_launch (CUDA events
- * on `stream`).  Overwrites rotating wavefield slots and the gradient
+ * virtual-source output -- the reverse reconstruction for plans with
+ * `reconstruct` --, 2 adjoint with gradient accumulation; 10, 11, 12 the
+ * two-step launches of the same modes for plans with time_block 2) for all
+ * shots and return the mean device time per launch in *ms_per_launch (CUDA
+ * events on `stream`).  Overwrites rotating wavefield slots and the gradient
  * accumulators, never the checkpoints; call after twi_forward. */
 int twi_plan_profile(twi_plan* plan, int mode, int repeats, float* ms_per_launch, void* stream);
 int twi_plan_destroy(twi_plan* plan);

@@ -159,3 +159,20 @@ def test_time_block_option_on_host():
     L.twi_plan_layout(h, ctypes.byref(lay))
     L.twi_plan_destroy(h)
     assert lay.time_block == 1
+
+
+def test_reconstruction_plan_trades_checkpoints_for_boundaries():
+    """Config-3 sizes: boundary saving needs a fraction of the checkpointed
+    plan's memory, and runs one step per launch."""
+    L = _capi.lib()
+    sizes = {}
+    for rec in (0, 1):
+        p = _problem(nt=6000, nshots=256, nx=1000, nz=300, ckpt_interval=50, reconstruct=rec)
+        n = ctypes.c_size_t()
+        assert L.twi_plan_footprint_bytes(ctypes.byref(p), ctypes.byref(n)) == 0
+        sizes[rec] = n.value
+    assert sizes[1] < 0.3 * sizes[0]
+    boundary = 2 * 2 * 300 + 2 * 1004
+    assert sizes[1] >= 6001 * 256 * boundary * 4
+    st, h = _create(reconstruct=1, time_block=2)
+    assert st == _capi.TWI_ERR_INVALID

@@ -116,8 +116,13 @@ __device__ __forceinline__ float keys_cell(float uo_a, float uo_b, float uo_c, f
 // Point-source / adjoint-source increment amp*v*v*dt^2, formed left to
 // right as in propagator_cpu.cpp:62 and :138.
 template <bool EXACT>
+__device__ __forceinline__ float injection(float amp, float v, float dt2) {
+    if constexpr (EXACT) return __fmul_rn(__fmul_rn(__fmul_rn(amp, v), v), dt2);
+    return amp * v * v * dt2;
+}
+template <bool EXACT>
 __device__ __forceinline__ float add_injection(float val, float amp, float v, float dt2) {
-    if constexpr (EXACT) return __fadd_rn(val, __fmul_rn(__fmul_rn(__fmul_rn(amp, v), v), dt2));
+    if constexpr (EXACT) return __fadd_rn(val, injection<EXACT>(amp, v, dt2));
     return fmaf(amp * v * v, dt2, val);
 }
 

@@ -16,6 +16,9 @@ enum StepMode : int {
                           // gradient term accumulated
     kModeExaForward = 3,  // forward step; the virtual source of largest
                           // magnitude and its step index kept per cell
+    kModeReverse = 4,     // u^{n-1} from u^n and u^{n+1} (the forward step run
+                          // backwards, source removed); pad cells restored
+                          // from the boundary buffer; virtual source written
 };
 
 // Gradient accumulator layout used by kModeAdjoint.
@@ -70,6 +73,11 @@ struct StepArgs {
     // excitation amplitude (modes 3 and kAccExa): per shot, same pitch/slot size
     float* exa;
     short* iexa;
+    // boundary saving: Keys cells of u^k, bnd[(k*nshots + s)*bnd_cells + idx]
+    // (idx in the boundary CTAs' cell order); written by kModeForward when
+    // set, read by kModeReverse
+    float* bnd;
+    int bnd_cells;
     int acc_mode;
     int acc_base;               // slot of group 0 / shot 0
     int* err;                   // device error word (bit 0: TMA wait timeout)

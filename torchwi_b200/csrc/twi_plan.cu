@@ -158,11 +158,13 @@ struct twi_plan {
     int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
     int tb = 1, rot = 3;   // time steps per launch (1 or 2) and rotation slots per role
     bool gradient = true, kahan = true, exa = false;
+    bool recon = false;     // boundary saving + reverse reconstruction instead of checkpoints
+    int nb = 0;             // boundary (Keys) cells per shot and time level
     long long nslots = 0, nvirt = 0, nacc = 0;
     // workspace regions (byte offsets)
     size_t off_vel = 0, off_wav = 0, off_frd = 0, off_grad = 0, off_coords = 0, off_err = 0,
            off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, off_exa = 0,
-           off_iexa = 0, off_mpart = 0, total = 0;
+           off_iexa = 0, off_mpart = 0, off_bnd = 0, total = 0;
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
@@ -196,7 +198,7 @@ struct twi_plan {
     // slot of u^k during the forward pass
     Slot fwd_slot(long long k, bool save) const {
         if (k <= 0) return zero();
-        if (save && gradient && !exa) {
+        if (save && gradient && !exa && !recon) {
             if (k % K == 0 && k / K < nseg) return ckpt((int)(k / K), 1);
             if ((k + 1) % K == 0 && (k + 1) / K < nseg) return ckpt((int)((k + 1) / K), 0);
         }
@@ -270,6 +272,10 @@ struct twi_plan {
             a.iexa = reinterpret_cast<short*>(ws + off_iexa);
             blocked = false;
         }
+        if (recon && save) {   // the Keys cells of every u^k go to the boundary buffer
+            a.bnd = F(off_bnd);
+            a.bnd_cells = nb;
+        }
         for (int it = 0; it < p.nt;) {
             const int n = blocked && it + 1 < p.nt ? 2 : 1;
             a.it = it;
@@ -302,8 +308,37 @@ struct twi_plan {
 
     // The gradient pass (without the accumulator reset and the final
     // reduction) as a list of launches: per segment, recompute then adjoint.
+    // Boundary saving: backwards from u^{nt}, u^{nt-1} (left by the forward
+    // pass), each step first rebuilds u^{it-1} and the virtual source of
+    // step it (kModeReverse, pad cells from the boundary buffer), then takes
+    // the adjoint step it.  u^0 = u^{-1} = 0 come from the zero slot.
+    void recon_gradient_steps(std::vector<Step>& out) const {
+        StepArgs a = base_args();
+        a.virt_out = F(off_virt);
+        a.virt_in = F(off_virt);
+        a.virt_stride = 1;
+        a.virt_base = 0;
+        a.resid = F(off_frd);
+        a.acc = F(off_acc);
+        a.acc_comp = kahan ? F(off_comp) : nullptr;
+        a.acc_mode = kahan ? kAccKahanPerGroup : kAccPlainPerShot;
+        a.acc_base = 0;
+        a.bnd = F(off_bnd);
+        a.bnd_cells = nb;
+        auto rslot = [&](long long k) { return k <= 0 ? zero() : urot((int)(k % 3)); };
+        for (int it = p.nt - 1; it >= 0; --it) {
+            a.it = it;
+            set_slots(a, rslot(it + 1), rslot(it), urot((it + 2) % 3), zero());
+            out.push_back({kModeReverse, a});
+            const long long m = (long long)p.nt - 1 - it;
+            set_slots(a, lam_slot(m - 2), lam_slot(m - 1), lam_slot(m), zero());
+            out.push_back({kModeAdjoint, a});
+        }
+    }
+
     void gradient_steps(std::vector<Step>& out, bool blocked) const {
         if (exa) return exa_gradient_steps(out);
+        if (recon) return recon_gradient_steps(out);
         StepArgs a = base_args();
         a.virt_out = F(off_virt);
         a.virt_in = F(off_virt);
@@ -466,11 +501,21 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
         delete P;
         return fail(TWI_ERR_INVALID, "time_block must be 0 (choose), 1 or 2");
     }
-    P->tb = P->exa ? 1 : p.time_block == 0 ? kDefaultTimeBlock : p.time_block;
+    P->recon = p.reconstruct != 0 && P->gradient && !P->exa;
+    if (P->recon && p.time_block == 2) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "reverse reconstruction runs one time step per launch");
+    }
+    P->tb = P->exa || P->recon ? 1 : p.time_block == 0 ? kDefaultTimeBlock : p.time_block;
     P->rot = P->tb == 2 ? 4 : 3;
-    P->sps = P->gradient ? 2 * P->rot + (P->exa ? 0 : 2 * (P->nseg - 1)) : P->rot;
+    if (P->recon) {   // no checkpoints: one segment, one virtual-source slot per shot
+        P->K = p.nt;
+        P->nseg = 1;
+    }
+    P->nb = 2 * P->ne * (P->dimz - 2 * P->ne) + P->ne * P->dimx;
+    P->sps = P->gradient ? 2 * P->rot + (P->exa || P->recon ? 0 : 2 * (P->nseg - 1)) : P->rot;
     P->nslots = 1 + (long long)p.nshots * P->sps;
-    P->nvirt = P->gradient && !P->exa ? (long long)p.nshots * K : 0;
+    P->nvirt = P->gradient && !P->exa ? (long long)p.nshots * (P->recon ? 1 : K) : 0;
     P->nacc = P->gradient ? (P->kahan ? P->ngroups : p.nshots) : 0;
 
     // workspace layout
@@ -491,6 +536,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->off_exa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 4 : 0);
     P->off_iexa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 2 : 0);
     P->off_mpart = take(P->gradient ? (size_t)kMisfitBlocks * sizeof(double) : 0);
+    P->off_bnd = take(P->recon ? (size_t)(p.nt + 1) * p.nshots * P->nb * 4 : 0);
     P->total = off;
     *out = P;
     return TWI_OK;
@@ -650,7 +696,7 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
     StepArgs a = P->base_args();
     const int it = P->p.nt / 2;
     a.it = it;
-    const StepMode m = static_cast<StepMode>(mode);
+    StepMode m = static_cast<StepMode>(mode);
     if (m == kModeAdjoint) {
         const Slot l0 = P->lrot(0), l1 = P->lrot(1), l2 = P->lrot(2), l3 = P->lrot(P->rot - 1);
         a.prev_base = l0.base, a.cur_base = l1.base, a.next_base = l2.base, a.next2_base = l3.base;
@@ -663,10 +709,15 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
         const Slot u0 = P->urot(0), u1 = P->urot(1), u2 = P->urot(2), u3 = P->urot(P->rot - 1);
         a.prev_base = u0.base, a.cur_base = u1.base, a.next_base = u2.base, a.next2_base = u3.base;
         if (m == kModeRecompute) a.virt_out = P->F(P->off_virt);
+        if (m == kModeRecompute && P->recon) {   // its gradient pass rebuilds backwards instead
+            m = kModeReverse;
+            a.bnd = P->F(P->off_bnd);
+            a.bnd_cells = P->nb;
+        }
     }
     a.prev_stride = a.cur_stride = a.next_stride = a.next2_stride = P->sps;
-    a.virt_stride = P->K;
-    a.virt_base = m == kModeAdjoint ? 1 : 0;   // two-step adjoint reads slots 1 and 0
+    a.virt_stride = P->recon ? 1 : P->K;
+    a.virt_base = m == kModeAdjoint && !P->recon ? 1 : 0;   // two-step adjoint reads slots 1 and 0
     cudaEvent_t e0, e1;
     TWI_CUDA(cudaEventCreate(&e0));
     TWI_CUDA(cudaEventCreate(&e1));
@@ -707,7 +758,7 @@ std::vector<twi_problem> tune_candidates(const twi_problem& p) {
         for (int rz : {4, 8}) {
             if (p.rows_per_warp && rz != p.rows_per_warp) continue;
             for (int tb : {1, 2}) {
-                if ((p.time_block && tb != p.time_block) || (p.exa && tb == 2)) continue;
+                if ((p.time_block && tb != p.time_block) || ((p.exa || p.reconstruct) && tb == 2)) continue;
                 twi_problem q = p;
                 q.nt = 8;
                 q.ckpt_interval = 2;
@@ -816,6 +867,7 @@ int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, in
     if (!P->ws) return fail(TWI_ERR_STATE, "bind the plan before submitting it");
     if (kind == 1 && !P->gradient) return fail(TWI_ERR_STATE, "a forward-only plan cannot take a gradient request");
     if (P->exa) return fail(TWI_ERR_INVALID, "excitation-amplitude plans run through twi_forward/twi_gradient only");
+    if (P->recon) return fail(TWI_ERR_INVALID, "reverse-reconstruction plans run through twi_forward/twi_gradient only");
     if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
     if (P->p.order != order || (P->p.exact != 0) != exact ||
         default_shape(P->rz).rows_per_warp != rows_per_warp)
@@ -958,9 +1010,10 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
             B->use_graphs = P->p.use_graphs != 0;
             B->shape = default_shape(P->rz);
         }
-        if (P->exa) {
+        if (P->exa || P->recon) {
             delete B;
-            return fail(TWI_ERR_INVALID, "excitation-amplitude plans run through twi_forward/twi_gradient only");
+            return fail(TWI_ERR_INVALID, "excitation-amplitude and reverse-reconstruction plans run through "
+                                         "twi_forward/twi_gradient only");
         }
         if (P->p.order != B->order || (P->p.exact != 0) != B->exact ||
                    default_shape(P->rz).rows_per_warp != B->shape.rows_per_warp) {

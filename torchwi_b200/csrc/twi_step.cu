@@ -98,14 +98,27 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
         }
         const long long cell = (long long)r * a.pitch + c;
         const float v = a.vel[cell];
-        const float q = (MODE == kModeRecompute || MODE == kModeExaForward) ? virt_coef<EXACT>(v, a.cons) : 0.f;
+        const float q = (MODE == kModeRecompute || MODE == kModeExaForward || MODE == kModeReverse)
+                            ? virt_coef<EXACT>(v, a.cons) : 0.f;
         for (int s = s0; s < s1; ++s) {
             const float* U2 = a.fields + (long long)(d.cur_base + s * d.cur_stride) * a.slot_elems + cell;
             const float* U1 = a.fields + (long long)(d.prev_base + s * d.prev_stride) * a.slot_elems + cell;
             const float uo = U2[0], um = U1[0];
-            const float out = keys_cell<EXACT>(uo, U2[db], U2[2 * db], um, U1[db], v, a.h2, a.dt2, a.hdt);
+            float out;
+            if constexpr (MODE == kModeReverse)   // u^{it-1} as the forward pass saved it (u^0 = 0)
+                out = d.it >= 2 ? a.bnd[((long long)(d.it - 1) * a.nshots + s) * a.bnd_cells + idx] : 0.f;
+            else
+                out = keys_cell<EXACT>(uo, U2[db], U2[2 * db], um, U1[db], v, a.h2, a.dt2, a.hdt);
             a.fields[(long long)(d.next_base + s * d.next_stride) * a.slot_elems + cell] = out;
-            if constexpr (MODE != kModeAdjoint) {
+            if constexpr (MODE == kModeForward) {
+                if (a.bnd != nullptr)
+                    a.bnd[((long long)(d.it + 1) * a.nshots + s) * a.bnd_cells + idx] = out;
+            }
+            if constexpr (MODE == kModeReverse) {   // um holds u^{it+1}, out u^{it-1}
+                a.virt_out[(long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                           (long long)r * a.virt_pitch + c] = virt_from_coef<EXACT>(q, out, uo, um);
+            }
+            if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
                 // a receiver row inside the bottom pad records Keys values
                 if (a.frd != nullptr && r == a.rec_row[s] && c >= NE && c < NE + a.nx) {
                     const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx + (c - NE);
@@ -223,7 +236,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     // per-cell constants over all shots: v*v*dt^2/h^2, and for the recompute
     // the virtual-source coefficient; v itself stays in shared memory
     float4 vvreg[RZ];
-    constexpr bool kVirt = MODE == kModeRecompute || MODE == kModeExaForward;
+    constexpr bool kVirt = MODE == kModeRecompute || MODE == kModeExaForward || MODE == kModeReverse;
     float4 qreg[kVirt ? RZ : 1];
 #pragma unroll
     for (int rr = 0; rr < RZ; ++rr) {
@@ -353,12 +366,14 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                                 g[m] = grad_term<EXACT>(a.exa[e0 + m], 0.f);
                     }
                 }
-                if constexpr (MODE == kModeRecompute) {
+                if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
                     if (col_ok) {
                         float vo[4];
 #pragma unroll
                         for (int m = 0; m < 4; ++m)
-                            vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
+                            vo[m] = MODE == kModeReverse
+                                        ? virt_from_coef<EXACT>(comp(qreg[rr], m), 0.f, c4[m], um[m])
+                                        : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
                         float* p = a.virt_out +
                                    (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                    (long long)r * a.virt_pitch + c;
@@ -373,6 +388,17 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                 }
             } else {
                 float out[4];
+                // backwards, u^{it+1} stands where u^{n-1} did, with the source
+                // that step `it` added taken off again
+                float ui[4] = {um[0], um[1], um[2], um[3]};
+                if constexpr (MODE == kModeReverse) {
+                    if (r == src_r && src_c >= c && src_c < c + 4) {
+                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+#pragma unroll
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m == src_c) ui[m] = __fsub_rn(um[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
+                    }
+                }
 #pragma unroll
                 for (int m = 0; m < 4; ++m) {
                     float lf[NE], rt[NE], up[NE], dn[NE];
@@ -384,11 +410,14 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         up[d - 1] = comp(win[NE - d], m);
                         dn[d - 1] = comp(win[NE + d], m);
                     }
-                    out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], um[m],
+                    out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
                                                            comp(vvreg[rr], m));
+                    if constexpr (MODE == kModeReverse) {
+                        if (d.it < 2) out[m] = 0.f;   // u^0 = u^{-1} = 0 exactly
+                    }
                 }
                 // sources land on interior cells only (validated on the host)
-                if constexpr (MODE != kModeAdjoint) {
+                if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
                     if (r == src_r && src_c >= c && src_c < c + 4) {
                         const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
@@ -396,7 +425,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                             if (c + m == src_c)
                                 out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
                     }
-                } else {
+                } else if constexpr (MODE == kModeAdjoint) {
                     if (r == rec_r) {
                         const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
                         const float* rs =
@@ -419,7 +448,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         if (cell_in[m]) dst[m] = out[m];
                 }
 
-                if constexpr (MODE != kModeAdjoint) {
+                if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
                     if (a.frd != nullptr && r == rec_r) {
                         const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
                         float* g = a.frd + o;
@@ -440,11 +469,13 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     }
                 }
 
-                if constexpr (MODE == kModeRecompute) {
+                if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
                     float vo[4];
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
-                        vo[m] = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                        vo[m] = MODE == kModeReverse
+                                    ? virt_from_coef<EXACT>(comp(qreg[rr], m), out[m], c4[m], um[m])
+                                    : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
                     float* p = a.virt_out +
                                (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                (long long)r * a.virt_pitch + c;
@@ -644,7 +675,7 @@ cudaError_t configure_one() {
     e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     if (e != cudaSuccess) return e;
-    if constexpr (MODE != kModeExaForward) {   // multi-plan kernels: modes 0-2
+    if constexpr (MODE <= kModeAdjoint) {   // multi-plan kernels: modes 0-2
         e = cudaFuncSetAttribute(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
         if (e != cudaSuccess) return e;
@@ -661,8 +692,8 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
     if (e != cudaSuccess || q.configure_only) return e;
     if (q.engine || q.multi) {
-        if constexpr (MODE == kModeExaForward) {
-            return cudaErrorInvalidValue;   // excitation amplitude: single-plan launches only
+        if constexpr (MODE > kModeAdjoint) {
+            return cudaErrorInvalidValue;   // excitation amplitude, reverse: single-plan launches only
         } else {
             if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
             if (q.engine)
@@ -696,6 +727,7 @@ cudaError_t launch_mode(StepMode mode, LaunchShape sh, const LaunchReq& q, cudaS
         case kModeRecompute: return launch_shape<ORDER, EXACT, kModeRecompute>(sh, q, st);
         case kModeAdjoint: return launch_shape<ORDER, EXACT, kModeAdjoint>(sh, q, st);
         case kModeExaForward: return launch_shape<ORDER, EXACT, kModeExaForward>(sh, q, st);
+        case kModeReverse: return launch_shape<ORDER, EXACT, kModeReverse>(sh, q, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -879,7 +911,7 @@ int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
 cudaError_t prepare_step(int order, bool exact, LaunchShape shape) {
     LaunchReq q;
     q.configure_only = true;
-    for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeExaForward}) {
+    for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeExaForward, kModeReverse}) {
         cudaError_t e = launch_req(order, exact, m, shape, q, nullptr);
         if (e != cudaSuccess) return e;
     }

@@ -41,6 +41,11 @@ class PlanOptions:
     time_block:  time steps per kernel launch in forward and gradient passes
                  (1 or 2; 0 = the library's choice).  Two steps read the
                  wavefields once per two steps; results are identical.
+    reconstruct: boundary saving instead of checkpoints: the forward pass keeps
+                 the absorbing-boundary cells of every step and the gradient
+                 pass rebuilds the wavefield backwards in time (much less
+                 memory; gradients within FP32 tolerance of the reference,
+                 not bit-identical).
     """
 
     exact: bool = True
@@ -52,6 +57,7 @@ class PlanOptions:
     forward_only: bool = False
     exa: bool = False
     time_block: int = 0
+    reconstruct: bool = False
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -82,7 +88,7 @@ def autotune(nx, nz, nshots, order=4, h=10.0, dt=1e-3, options: PlanOptions | No
     o = options or PlanOptions()
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     key = (dev.index, nx, nz, nshots, order, o.exact, o.accumulate, o.forward_only, o.exa,
-           o.shots_per_cta, o.rows_per_warp, o.time_block)
+           o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct)
     if key in _TUNED:
         return _TUNED[key]
     import dataclasses
@@ -127,7 +133,7 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
                    use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
                    forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)),
-                   time_block=int(o.time_block))
+                   time_block=int(o.time_block), reconstruct=int(bool(o.reconstruct)))
 
 
 class ShotPlan:
