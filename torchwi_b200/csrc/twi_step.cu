@@ -583,6 +583,16 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     }
 }
 
+// Copy one job's arguments into shared memory (all threads take part; the
+// body's first barrier orders the copy before any use).
+__device__ __forceinline__ void copy_args(StepArgs& dst, const StepArgs& src) {
+    static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied in 4-byte words");
+    const int* s = reinterpret_cast<const int*>(&src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / 4); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
@@ -607,8 +617,20 @@ step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
     }
     const MultiJob& J = jobs[lo];
     const CUtensorMap* tm = tmaps + 3 * J.plan;
-    const StepDyn d = dyn_of(J.a);
-    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, d, J.nbc, blockIdx.x - J.cta_begin);
+    // Read through a pointer into global memory, the arguments would have to
+    // be re-read from there after the kernel's own global stores.  The
+    // forward step copies them into registers; the recompute and adjoint
+    // steps, which hold more live values, into shared memory.
+    if constexpr (MODE == kModeForward) {
+        const StepArgs a = J.a;
+        step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, a, dyn_of(a), J.nbc,
+                                              blockIdx.x - J.cta_begin);
+    } else {
+        __shared__ StepArgs a;
+        copy_args(a, J.a);
+        step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, a, dyn_of(a), J.nbc,
+                                              blockIdx.x - J.cta_begin);
+    }
 }
 
 // Engine launches: the CTA ranges and the per-step integers come from the
@@ -625,8 +647,16 @@ step_kernel_engine(const __grid_constant__ EngineLaunch L, const CUtensorMap* __
     }
     const MultiJob& J = *L.tmpl[lo];
     const CUtensorMap* tm = tmaps + 3 * J.plan;
-    step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, J.a, L.dyn[lo], J.nbc,
-                                          blockIdx.x - L.cta_begin[lo]);
+    if constexpr (MODE == kModeForward) {   // arguments copied as in step_kernel_multi
+        const StepArgs a = J.a;
+        step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, a, L.dyn[lo], J.nbc,
+                                              blockIdx.x - L.cta_begin[lo]);
+    } else {
+        __shared__ StepArgs a;
+        copy_args(a, J.a);
+        step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, a, L.dyn[lo], J.nbc,
+                                              blockIdx.x - L.cta_begin[lo]);
+    }
 }
 
 // ---------------------------------------------------------------------------
