@@ -121,6 +121,17 @@ def cpu_reference_shot_gradient(survey, k):
     return time.perf_counter() - t0
 
 
+ONE_THREAD_NT = 400
+
+
+def cpu_one_thread_seconds():
+    """Seconds of one config-2 shot-gradient with nt=ONE_THREAD_NT on one
+    thread (run in a child process with OMP_NUM_THREADS=1)."""
+    from torchwi_b200 import synthetic
+    short = synthetic.config2(nshots=64, nt=ONE_THREAD_NT)
+    return cpu_reference_shot_gradient(short, 31)
+
+
 def cpu_baseline(survey, nsample=1):
     import oracle as O
 
@@ -129,9 +140,20 @@ def cpu_baseline(survey, nsample=1):
         return None
     cores = os.cpu_count() or 1
     secs = [cpu_reference_shot_gradient(survey, 31 + i) for i in range(nsample)]
-    return {"value": nsample / sum(secs), "unit": "shot-gradients/s", "cores": cores, "kind": kind,
-            "sample": f"{nsample} shot-gradient(s) of the 1000x300 nt=4000 survey "
-                      f"(forward + adjoint, reference CPU propagator, OMP_NUM_THREADS={cores})"}
+    out = {"value": nsample / sum(secs), "unit": "shot-gradients/s", "cores": cores, "kind": kind,
+           "sample": f"{nsample} shot-gradient(s) of the 1000x300 nt=4000 survey "
+                     f"(forward + adjoint, reference CPU propagator, OMP_NUM_THREADS={cores})"}
+    try:   # the same on one thread, on a shorter run scaled by nt
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        code = f"import sys; sys.path.insert(0, {REPO!r}); import bench; print(bench.cpu_one_thread_seconds())"
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        t1 = float(r.stdout.strip().splitlines()[-1]) * (survey.nt / ONE_THREAD_NT)
+        out["one_thread"] = {"value": 1.0 / t1, "unit": "shot-gradients/s", "cores": 1,
+                             "sample": f"one shot-gradient with nt={ONE_THREAD_NT}, time scaled "
+                                       f"linearly to nt={survey.nt}"}
+    except Exception as e:   # reported, not fatal
+        out["one_thread"] = {"unavailable": str(e)[:200]}
+    return out
 
 
 def run_reference(args):
