@@ -205,6 +205,14 @@ int twi_plan_check(twi_plan* plan, void* stream);
  * accumulators, never the checkpoints; call after twi_forward. */
 int twi_plan_profile(twi_plan* plan, int mode, int repeats, float* ms_per_launch, void* stream);
 int twi_plan_destroy(twi_plan* plan);
+/* Diagnostics (no counterpart in the reference).  Every wait in the kernels
+ * is bounded in time; when one runs out the kernel raises the device error
+ * word (TWI_ERR_DEVICE from twi_plan_check), waits for its own copies in
+ * flight and returns, leaving the context usable.  This launches a kernel
+ * whose wait can never complete (nothing arrives at its barrier) with a
+ * limit of `limit_us` microseconds and returns TWI_OK when the wait ran out
+ * and was reported as designed; *elapsed_ms gets the kernel's duration. */
+int twi_check_wait_timeout(int limit_us, float* elapsed_ms, void* stream);
 /* Workspace bytes a plan of `prob` needs (host only; admission control). */
 int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes);
 

@@ -43,13 +43,39 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return done != 0;
 }
 
-// Wait with an iteration limit; returns false (and the caller raises the
-// device error flag and leaves) if the copies never land.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
-    constexpr uint32_t kMaxProbes = 1u << 24;
-    for (uint32_t i = 0; i < kMaxProbes; ++i)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait at most `limit_ns` of wall time (checked every 256 probes, with a
+// probe count as a second bound in case the timer does not advance);
+// returns false if the phase never completes.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
+    constexpr uint32_t kMaxProbes = 1u << 26;
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 0; i < kMaxProbes; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255u) == 255u && globaltimer_ns() - t0 > limit_ns) return false;
+    }
     return false;
+}
+
+// The step kernels' wait: a copy of a few tens of KB lands in microseconds,
+// so two seconds only runs out when something is broken; the caller then
+// raises the device error word, drains its other copies and leaves.
+constexpr uint64_t kWaitLimitNs = 2000000000ull;
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+    return mbar_wait_for(bar, parity, kWaitLimitNs);
+}
+
+// After a wait ran out: wait, bounded again, for the stage copies of shots
+// [first, last) that this CTA issued (stage barrier j % stages, phase
+// (j / stages) & 1), so that none lands in shared memory the CTA gave back.
+__device__ __forceinline__ void drain_stages(uint64_t* stage_bars, int stages, int first, int last) {
+    for (int j = first; j < last; ++j)
+        mbar_wait_for(&stage_bars[j % stages], (uint32_t)((j / stages) & 1), kWaitLimitNs);
 }
 
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm) {

@@ -229,7 +229,10 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
         if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(a.err, 1);
+            if (threadIdx.x == 0) {
+                atomicOr(a.err, 1);
+                drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
+            }
             return;
         }
     }
@@ -313,7 +316,10 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         {
             const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicOr(a.err, 1);
+                if (threadIdx.x == 0) {
+                    atomicOr(a.err, 1);
+                    drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
+                }
                 return;
             }
         }
@@ -403,12 +409,12 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                 for (int m = 0; m < 4; ++m) {
                     float lf[NE], rt[NE], up[NE], dn[NE];
 #pragma unroll
-                    for (int d = 1; d <= NE; ++d) {
-                        const int jl = m - d, jr = m + d;
-                        lf[d - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
-                        rt[d - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
-                        up[d - 1] = comp(win[NE - d], m);
-                        dn[d - 1] = comp(win[NE + d], m);
+                    for (int dist = 1; dist <= NE; ++dist) {
+                        const int jl = m - dist, jr = m + dist;
+                        lf[dist - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
+                        rt[dist - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
+                        up[dist - 1] = comp(win[NE - dist], m);
+                        dn[dist - 1] = comp(win[NE + dist], m);
                     }
                     out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
                                                            comp(vvreg[rr], m));

@@ -140,7 +140,7 @@ __device__ __forceinline__ void step2_body(const CUtensorMap& tm_un, const CUten
                                            const CUtensorMap& tm_v, const StepArgs& a, int x0,
                                            int z0, int grp) {
     using S = Smem2<ORDER, RZ, WZ>;
-    constexpr int NE = S::NE, TZ = S::TZ, RING = S::RING, RA = S::RA, RAW = S::RAW, STAGES = S::STAGES;
+    constexpr int NE = S::NE, RING = S::RING, RA = S::RA, RAW = S::RAW, STAGES = S::STAGES;
     constexpr int DIR = MODE == kModeAdjoint ? -1 : 1;
     const int s_begin = grp * a.spc;
     const int nloc = min(a.spc, a.nshots - s_begin);
@@ -188,7 +188,10 @@ __device__ __forceinline__ void step2_body(const CUtensorMap& tm_un, const CUten
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
         if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) atomicOr(a.err, 1);
+            if (threadIdx.x == 0) {
+                atomicOr(a.err, 1);
+                drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
+            }
             return;
         }
     }
@@ -242,7 +245,10 @@ __device__ __forceinline__ void step2_body(const CUtensorMap& tm_un, const CUten
         {
             const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
             if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) atomicOr(a.err, 1);
+                if (threadIdx.x == 0) {
+                    atomicOr(a.err, 1);
+                    drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
+                }
                 return;
             }
         }
