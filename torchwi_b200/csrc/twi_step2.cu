@@ -256,14 +256,15 @@ __device__ __forceinline__ void step2_body(const CUtensorMap& tm_un, const CUten
         // ---- step A: u^{n+1} on the output tile plus its NE ring ----------
         {
             const int ra0 = warp * RAW;
-            float4 win[2 * NE + 1];
-#pragma unroll
-            for (int j = 0; j < 2 * NE; ++j) win[j] = ld4(un + (ra0 + j) * kUnX + cs);
-#pragma unroll
+            // a rolled loop (the stencil rows are re-read from shared memory
+            // each row) keeps the kernel's code small
+#pragma unroll 1
             for (int i = 0; i < RAW; ++i) {
                 const int ra = ra0 + i;
                 if (ra >= RA) break;                      // warp-uniform
-                win[2 * NE] = ld4(un + (ra + 2 * NE) * kUnX + cs);
+                float4 win[2 * NE + 1];
+#pragma unroll
+                for (int j = 0; j <= 2 * NE; ++j) win[j] = ld4(un + (ra + j) * kUnX + cs);
                 const int r = z0 - RING + ra;
                 const float* urow = un + (ra + NE) * kUnX;
                 float L[NE], R[NE];
@@ -307,8 +308,6 @@ __device__ __forceinline__ void step2_body(const CUtensorMap& tm_un, const CUten
                     }
                 }
                 *reinterpret_cast<float4*>(As + ra * kRegX + ca) = make_float4(out[0], out[1], out[2], out[3]);
-#pragma unroll
-                for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
             }
         }
         __syncthreads();   // step A complete: As holds u^{n+1}
