@@ -18,6 +18,7 @@
 // float4s along z, and warp shuffles for the x neighbours (lanes 0 and 31
 // read the x halo from shared memory).  Rows/columns of the pads use the
 // general per-cell path.  The top NE rows are the free surface: always 0.
+#include <atomic>
 #include <cstdio>
 
 #include "twi_cell.cuh"
@@ -703,11 +704,13 @@ int ctas_of(const StepArgs& a, int* nbc_out) {
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 cudaError_t configure_one() {
     using S = Smem<ORDER, RZ, WZ>;
-    static unsigned long long configured = 0;   // one bit per device
+    // one bit per device; setting an attribute twice is harmless, but plans
+    // may be created from several host threads
+    static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev >= 64 || (configured & (1ull << dev))) return cudaSuccess;
+    if (dev >= 64 || (configured.load(std::memory_order_relaxed) & (1ull << dev))) return cudaSuccess;
     e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     if (e != cudaSuccess) return e;
@@ -718,7 +721,7 @@ cudaError_t configure_one() {
         e = cudaFuncSetAttribute(step_kernel_engine<ORDER, EXACT, MODE, RZ, WZ>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     }
-    if (e == cudaSuccess) configured |= 1ull << dev;
+    if (e == cudaSuccess) configured.fetch_or(1ull << dev, std::memory_order_relaxed);
     return e;
 }
 

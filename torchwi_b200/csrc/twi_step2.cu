@@ -27,6 +27,7 @@
 // next (step A) and next2 (step B); the planner gives the four distinct
 // slots.  The virtual-source slot of step B is virt_base + 1 (forward
 // direction) or virt_base - 1 (adjoint).
+#include <atomic>
 #include <cstdio>
 
 #include "twi_cell.cuh"
@@ -508,15 +509,17 @@ template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 cudaError_t launch2_one(const CUtensorMap& tun, const CUtensorMap& tum, const CUtensorMap& tv,
                         const StepArgs& a, bool configure_only, cudaStream_t stream) {
     using S = Smem2<ORDER, RZ, WZ>;
-    static unsigned long long configured = 0;   // one bit per device
+    // one bit per device; setting an attribute twice is harmless, but plans
+    // may be created from several host threads
+    static std::atomic<unsigned long long> configured{0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 64 && !(configured & (1ull << dev))) {
+    if (dev < 64 && !(configured.load(std::memory_order_relaxed) & (1ull << dev))) {
         e = cudaFuncSetAttribute(step2_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
         if (e != cudaSuccess) return e;
-        configured |= 1ull << dev;
+        configured.fetch_or(1ull << dev, std::memory_order_relaxed);
     }
     if (configure_only) return cudaSuccess;
     const long long n = step2_ctas(ORDER, RZ, a);
