@@ -4,6 +4,7 @@ with the interface of TorchWI's time operator.
 Public API (mirrors torchwi.operator / torchwi.propagator):
     Time2d, Time2dForward        reference-compatible modules
     Time2dBatch                  all shots of a survey in one plan
+    Time2dModels                 several models of different sizes in one batch
     ShotPlan, PlanOptions        the underlying C-ABI plan
     autotune                     fastest launch shape for a grid and shot count
     inversion.Inversion          FWI driver over the batched plan
@@ -15,7 +16,7 @@ The CUDA library (torchwi_b200/_lib/libtwi_b200.so) is loaded on first use;
 build it with ``python -m torchwi_b200.build``.
 """
 
-from .operator import Time2d, Time2dBatch, Time2dForward  # noqa: F401
+from .operator import Time2d, Time2dBatch, Time2dForward, Time2dModels  # noqa: F401
 from .plan import PlanBatch, PlanOptions, ShotPlan, autotune, footprint_bytes  # noqa: F401
 from .source import fdgaus, ricker  # noqa: F401
 from ._capi import TwiError, TwiInvalid  # noqa: F401

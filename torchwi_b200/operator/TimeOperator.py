@@ -143,3 +143,77 @@ class _BatchOperator(torch.autograd.Function):
             m.plan.set_shots(*ctx.coords)
             m.plan.forward(save_checkpoints=True)
         return m.plan.gradient(grad_output).clone(), None
+
+
+class Time2dModels(torch.nn.Module):
+    """Several velocity models of different grid sizes, each with its own
+    shots (and its own nt), advanced together: every time step of all of
+    them is one launch per kernel mode (a PlanBatch).  Backward gives each
+    model its shot-summed gradient.
+
+        m = Time2dModels([(nx0, nz0), (nx1, nz1)], h, [w0, w1], dt, order, [S0, S1], device)
+        frd0, frd1 = m([vel0, vel1], [(sx0, sy0, ry0), (sx1, sy1, ry1)])
+        (loss(frd0) + loss(frd1)).backward()       # vel0.grad, vel1.grad
+
+    `w` is one wavelet for all models or a list (each (nt,) or (S_i, nt));
+    `h`, `dt` and `order` are shared.  Results equal running each model
+    alone (Time2dBatch), bit for bit."""
+
+    def __init__(self, shapes, h, w, dt, order, nshots, device="cuda",
+                 options: PlanOptions | None = None):
+        super().__init__()
+        from ..plan import PlanBatch
+        dev = TimeFunction._check_device(device)
+        if dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        shapes = [(int(a), int(b)) for a, b in shapes]
+        nshots = [int(n) for n in nshots]
+        if len(nshots) != len(shapes):
+            raise ValueError("one shot count per model")
+        ws = list(w) if isinstance(w, (list, tuple)) else [w] * len(shapes)
+        if len(ws) != len(shapes):
+            raise ValueError("one wavelet per model (or one for all)")
+        self.plans = []
+        for (nx, nz), ns, wi in zip(shapes, nshots, ws):
+            wi = torch.as_tensor(wi).detach().to(torch.float32)
+            p = ShotPlan(nx, nz, h, dt, int(wi.shape[-1]), order, nshots=ns,
+                         wavelet_per_shot=(wi.dim() == 2), options=options, device=dev)
+            p.set_wavelet(wi)
+            self.plans.append(p)
+        self.batch = PlanBatch(self.plans)
+        self._token = 0
+
+    def forward(self, vels, coords):
+        if len(vels) != len(self.plans) or len(coords) != len(self.plans):
+            raise ValueError("one velocity model and one (sx, sy, ry) per model")
+        return _ModelsOperator.apply(self, tuple(tuple(c) for c in coords), *vels)
+
+
+class _ModelsOperator(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, m, coords, *vels):
+        m._token += 1
+        for p, v, c in zip(m.plans, vels, coords):
+            p.set_model(v)
+            p.set_shots(*c)
+        frds = m.batch.forward(save_checkpoints=True)
+        ctx.m, ctx.coords, ctx.token = m, coords, m._token
+        ctx.save_for_backward(*[v.detach() for v in vels])
+        return tuple(f.clone() for f in frds)
+
+    @staticmethod
+    def backward(ctx, *grad_outputs):
+        vels = ctx.saved_tensors
+        m = ctx.m
+        if m._token != ctx.token:   # another forward reused the plans since
+            for p, v, c in zip(m.plans, vels, ctx.coords):
+                p.set_model(v)
+                p.set_shots(*c)
+            m.batch.forward(save_checkpoints=True)
+        for p, g in zip(m.plans, grad_outputs):
+            if g is None:
+                p.resid.zero_()
+            else:
+                p.resid.copy_(g.detach().to(p.device, torch.float32).reshape(p.resid.shape))
+        grads = m.batch.gradient()
+        return (None, None) + tuple(g.clone() for g in grads)

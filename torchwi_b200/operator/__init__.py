@@ -1,1 +1,1 @@
-from .TimeOperator import Time2d, Time2dBatch, Time2dForward  # noqa: F401
+from .TimeOperator import Time2d, Time2dBatch, Time2dForward, Time2dModels  # noqa: F401
