@@ -78,6 +78,11 @@ __device__ __forceinline__ void drain_stages(uint64_t* stage_bars, int stages, i
         mbar_wait_for(&stage_bars[j % stages], (uint32_t)((j / stages) & 1), kWaitLimitNs);
 }
 
+// Bring the 128-byte line holding `p` into L2 (no register result).
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+    asm volatile("prefetch.L2 [%0];" ::"l"(reinterpret_cast<uint64_t>(p)) : "memory");
+}
+
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* tm) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(tm)) : "memory");
 }

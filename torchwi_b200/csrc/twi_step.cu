@@ -227,6 +227,20 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
 #pragma unroll
     for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
 
+    // the first shot's virtual source into L2 while the tiles load (the
+    // loop below prefetches each next shot's)
+    if constexpr (MODE == kModeAdjoint) {
+        if (nloc > 0 && (lane & 7) == 0 &&
+            (a.acc_mode == kAccKahanPerGroup || a.acc_mode == kAccPlainPerShot)) {
+            const float* nb = a.virt_in + (long long)(d.virt_base + s_begin * a.virt_stride) * a.virt_slot_elems;
+#pragma unroll
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int r = z0 + rl0 + rr;
+                if (col_ok && r < a.dimz) prefetch_l2(nb + (long long)r * a.virt_pitch + c);
+            }
+        }
+    }
+
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
         if (__syncthreads_or(!ok)) {
@@ -310,6 +324,19 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         if (c + 2 < a.dimx) vin[rr].z = p[2];
                         if (c + 3 < a.dimx) vin[rr].w = p[3];
                     }
+                }
+            }
+        }
+        // the next shot's virtual source into L2 while this one computes
+        // (one prefetch per 128-byte line of each warp row)
+        if constexpr (MODE == kModeAdjoint) {
+            if (k + 1 < nloc && (lane & 7) == 0 &&
+                (a.acc_mode == kAccKahanPerGroup || a.acc_mode == kAccPlainPerShot)) {
+                const float* nb = a.virt_in + (long long)(d.virt_base + (s + 1) * a.virt_stride) * a.virt_slot_elems;
+#pragma unroll
+                for (int rr = 0; rr < RZ; ++rr) {
+                    const int r = z0 + rl0 + rr;
+                    if (col_ok && r < a.dimz) prefetch_l2(nb + (long long)r * a.virt_pitch + c);
                 }
             }
         }
