@@ -128,7 +128,7 @@ typedef struct twi_problem {
                              1: plain FP32 per shot, summed in shot order (the
                              reference's order: bit-identical gradients) */
     int shots_per_cta;    /* shots sharing one velocity tile in a CTA; 0 = choose */
-    int rows_per_warp;    /* 4 or 8; 0 = choose */
+    int rows_per_warp;    /* 2, 4 or 8 (2: not with time_block 2); 0 = choose */
     int use_graphs;       /* 1: capture the time loops into CUDA graphs */
     int wavelet_per_shot; /* 1: wavelet region is [nshots][nt]; 0: one [nt] */
     int forward_only;     /* 1: no checkpoint, virtual-source or gradient memory;

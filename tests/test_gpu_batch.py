@@ -23,11 +23,12 @@ def _plan(s, opts):
     return p
 
 
-@pytest.mark.parametrize("accumulate", ["plain", "kahan"])
-@pytest.mark.parametrize("graphs", [True, False])
-def test_batch_equals_plans_alone(accumulate, graphs):
+@pytest.mark.parametrize("accumulate,graphs,rz", [("plain", True, 0), ("plain", False, 0),
+                                                  ("kahan", True, 0), ("kahan", False, 0),
+                                                  ("kahan", True, 2)])
+def test_batch_equals_plans_alone(accumulate, graphs, rz):
     surveys = [synthetic.small_case(order=4, **c) for c in CASES]
-    opts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs)
+    opts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs, rows_per_warp=rz)
     alone = []
     for s in surveys:
         p = _plan(s, opts)

@@ -206,12 +206,12 @@ int twi_engine_create(int order, int exact, int rows_per_warp, int max_requests,
     if (order != 2 && order != 4 && order != 8) return efail(TWI_ERR_INVALID, "order must be 2, 4 or 8");
     if (max_requests < 1 || max_requests > 4096)
         return efail(TWI_ERR_INVALID, "max_requests must be in [1, 4096]");
-    if (rows_per_warp != 0 && rows_per_warp != 4 && rows_per_warp != 8)
-        return efail(TWI_ERR_INVALID, "rows_per_warp must be 0, 4 or 8");
+    if (rows_per_warp != 0 && rows_per_warp != 2 && rows_per_warp != 4 && rows_per_warp != 8)
+        return efail(TWI_ERR_INVALID, "rows_per_warp must be 0, 2, 4 or 8");
     twi_engine* E = new twi_engine();
     E->order = order;
     E->exact = exact != 0;
-    E->shape = LaunchShape{rows_per_warp == 8 ? 8 : 4, 4};
+    E->shape = LaunchShape{rows_per_warp == 8 || rows_per_warp == 2 ? rows_per_warp : 4, 4};
     E->max_requests = max_requests;
     size_t off = 0;
     auto take = [&](size_t b) { size_t o = off; off = (off + b + 255) & ~size_t(255); return o; };

@@ -142,7 +142,7 @@ int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, in
 constexpr int kDefaultTimeBlock = 1;
 
 LaunchShape default_shape(int rows_per_warp) {
-    return LaunchShape{rows_per_warp == 8 ? 8 : 4, 4};
+    return LaunchShape{rows_per_warp == 8 || rows_per_warp == 2 ? rows_per_warp : 4, 4};
 }
 
 }  // namespace
@@ -465,8 +465,10 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     if (p.nx < 1 || p.nz < 1 || p.nt < 1 || p.nshots < 1)
         return fail(TWI_ERR_INVALID, "nx, nz, nt and nshots must be positive");
     if (!(p.h > 0.f) || !(p.dt > 0.f)) return fail(TWI_ERR_INVALID, "h and dt must be positive");
-    if (p.rows_per_warp != 0 && p.rows_per_warp != 4 && p.rows_per_warp != 8)
-        return fail(TWI_ERR_INVALID, "rows_per_warp must be 0, 4 or 8");
+    if (p.rows_per_warp != 0 && p.rows_per_warp != 2 && p.rows_per_warp != 4 && p.rows_per_warp != 8)
+        return fail(TWI_ERR_INVALID, "rows_per_warp must be 0, 2, 4 or 8");
+    if (p.rows_per_warp == 2 && p.time_block == 2)
+        return fail(TWI_ERR_INVALID, "two time steps per launch need rows_per_warp 4 or 8");
     if (p.ckpt_interval < 0 || p.ckpt_interval == 1)
         return fail(TWI_ERR_INVALID, "ckpt_interval must be 0 (choose) or >= 2");
 
@@ -749,16 +751,18 @@ namespace {
 
 // The launch shapes the autotuner tries for `prob`: every combination the
 // caller left open (0) of shots per CTA {1, 2, 4, 8} (at most nshots), rows
-// per warp {4, 8} and time steps per launch {1, 2} (1 for excitation
-// amplitude), each timed on a copy of the problem with nt = 8.
+// per warp {2, 4, 8} and time steps per launch {1, 2} (1 for excitation
+// amplitude, reverse reconstruction and 2 rows per warp), each timed on a
+// copy of the problem with nt = 8.
 std::vector<twi_problem> tune_candidates(const twi_problem& p) {
     std::vector<twi_problem> out;
     for (int spc : {1, 2, 4, 8}) {
         if (p.shots_per_cta ? spc != p.shots_per_cta : spc > std::max(1, p.nshots)) continue;
-        for (int rz : {4, 8}) {
+        for (int rz : {2, 4, 8}) {
             if (p.rows_per_warp && rz != p.rows_per_warp) continue;
             for (int tb : {1, 2}) {
-                if ((p.time_block && tb != p.time_block) || ((p.exa || p.reconstruct) && tb == 2)) continue;
+                if ((p.time_block && tb != p.time_block) || ((p.exa || p.reconstruct || rz == 2) && tb == 2))
+                    continue;
                 twi_problem q = p;
                 q.nt = 8;
                 q.ckpt_interval = 2;

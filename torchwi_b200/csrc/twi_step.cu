@@ -30,6 +30,10 @@ namespace {
 
 constexpr int round32(int n) { return (n + 31) / 32 * 32; }
 
+// CTAs per SM the launch bounds ask for: 2 rows per warp -> 5, 4 -> 4, 8 -> 2
+// (the 8-row tiles are held to 2 by shared memory)
+constexpr int kMinCtasPerSm(int rz) { return rz == 2 ? 5 : rz == 4 ? 4 : 2; }
+
 template <int ORDER, int RZ, int WZ>
 struct Smem {
     static constexpr int NE = ORDER / 2;
@@ -628,7 +632,7 @@ __device__ __forceinline__ void copy_args(StepArgs& dst, const StepArgs& src) {
 }
 
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+__global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
             const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ StepArgs a,
             const int nbc) {
@@ -640,7 +644,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 // ranges of the jobs are contiguous and ascending in jobs[].cta_begin; the
 // tensor maps of plan p are tmaps[3p .. 3p+2].
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+__global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
 step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
                   const CUtensorMap* __restrict__ tmaps) {
     int lo = 0, hi = njobs - 1;
@@ -671,7 +675,7 @@ step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
 // kernel parameters, the static arguments of each request and kernel mode
 // from a template resident in device memory.
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32, RZ == 4 ? 4 : 2)
+__global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
 step_kernel_engine(const __grid_constant__ EngineLaunch L, const CUtensorMap* __restrict__ tmaps) {
     int lo = 0, hi = L.njobs - 1;
     while (lo < hi) {
@@ -781,6 +785,7 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
 
 template <int ORDER, bool EXACT, int MODE>
 cudaError_t launch_shape(LaunchShape sh, const LaunchReq& q, cudaStream_t st) {
+    if (sh.warps == 4 && sh.rows_per_warp == 2) return launch_one<ORDER, EXACT, MODE, 2, 4>(q, st);
     if (sh.warps == 4 && sh.rows_per_warp == 4) return launch_one<ORDER, EXACT, MODE, 4, 4>(q, st);
     if (sh.warps == 4 && sh.rows_per_warp == 8) return launch_one<ORDER, EXACT, MODE, 8, 4>(q, st);
     return cudaErrorInvalidValue;
@@ -965,11 +970,11 @@ cudaError_t launch_step_engine(int order, bool exact, StepMode mode, LaunchShape
 }
 
 int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
-    const bool r8 = shape.rows_per_warp == 8;
+    const int rz = shape.rows_per_warp;
     switch (order) {
-        case 2: return r8 ? ctas_of<2, 8, 4>(a, nbc) : ctas_of<2, 4, 4>(a, nbc);
-        case 4: return r8 ? ctas_of<4, 8, 4>(a, nbc) : ctas_of<4, 4, 4>(a, nbc);
-        case 8: return r8 ? ctas_of<8, 8, 4>(a, nbc) : ctas_of<8, 4, 4>(a, nbc);
+        case 2: return rz == 8 ? ctas_of<2, 8, 4>(a, nbc) : rz == 2 ? ctas_of<2, 2, 4>(a, nbc) : ctas_of<2, 4, 4>(a, nbc);
+        case 4: return rz == 8 ? ctas_of<4, 8, 4>(a, nbc) : rz == 2 ? ctas_of<4, 2, 4>(a, nbc) : ctas_of<4, 4, 4>(a, nbc);
+        case 8: return rz == 8 ? ctas_of<8, 8, 4>(a, nbc) : rz == 2 ? ctas_of<8, 2, 4>(a, nbc) : ctas_of<8, 4, 4>(a, nbc);
     }
     return -1;
 }
