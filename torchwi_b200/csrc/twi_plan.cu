@@ -140,6 +140,10 @@ int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, in
 
 // Time steps per launch when the problem leaves it open.
 constexpr int kDefaultTimeBlock = 1;
+// Rows per warp when the problem leaves it open: 4 for the forward-type
+// steps, 2 for the adjoint (whose Kahan pairs and virtual-source window halve
+// with the rows, so 5 CTAs fit an SM).  An explicit value applies to all.
+constexpr int kDefaultAdjointRows = 2;
 
 LaunchShape default_shape(int rows_per_warp) {
     return LaunchShape{rows_per_warp == 8 || rows_per_warp == 2 ? rows_per_warp : 4, 4};
@@ -156,6 +160,7 @@ struct twi_plan {
     int ne = 0, dimx = 0, dimz = 0, pitch = 0;
     long long slot_elems = 0;
     int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
+    int rz_adj = 4;         // rows per warp of single-step adjoint launches
     int tb = 1, rot = 3;   // time steps per launch (1 or 2) and rotation slots per role
     bool gradient = true, kahan = true, exa = false;
     bool recon = false;     // boundary saving + reverse reconstruction instead of checkpoints
@@ -168,6 +173,7 @@ struct twi_plan {
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
+    CUtensorMap ta_u2{}, ta_u1{}, ta_vel{};    // adjoint launches when rz_adj != rz
     CUtensorMap tm2_un{}, tm2_um{}, tm2_v{};   // two-step launches
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t g_fwd[2] = {nullptr, nullptr};
@@ -244,9 +250,11 @@ struct twi_plan {
     }
 
     int launch(StepMode mode, const StepArgs& a, cudaStream_t st, int nsteps = 1) const {
+        const bool adj = nsteps == 1 && mode == kModeAdjoint && rz_adj != rz;
         cudaError_t e = nsteps == 2
             ? launch_step2(p.order, p.exact != 0, mode, default_shape(rz), tm2_un, tm2_um, tm2_v, a, st)
-            : launch_step(p.order, p.exact != 0, mode, default_shape(rz), tm_u2, tm_u1, tm_vel, a, st);
+            : adj ? launch_step(p.order, p.exact != 0, mode, default_shape(rz_adj), ta_u2, ta_u1, ta_vel, a, st)
+                  : launch_step(p.order, p.exact != 0, mode, default_shape(rz), tm_u2, tm_u1, tm_vel, a, st);
         if (e != cudaSuccess)
             return fail(TWI_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
         return TWI_OK;
@@ -490,6 +498,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     // shot (the adjoint writes acc + s * slot), summed in shot order
     if (P->exa) P->kahan = false;
     P->rz = p.rows_per_warp ? p.rows_per_warp : 4;
+    P->rz_adj = p.rows_per_warp ? p.rows_per_warp : kDefaultAdjointRows;
     int K = p.ckpt_interval;
     if (K == 0) K = std::max(2, (int)std::lround(std::sqrt(2.0 * p.nt)));
     K = std::min(K, std::max(2, p.nt));
@@ -560,6 +569,7 @@ int twi_plan_layout(const twi_plan* P, twi_layout* out) {
     out->nsegments = P->nseg;
     out->shots_per_cta = P->spc;
     out->rows_per_warp = P->rz;
+    out->adjoint_rows_per_warp = P->rz_adj;
     return TWI_OK;
 }
 
@@ -580,6 +590,15 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
     TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
                      TZ));
     TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
+    if (P->gradient && P->rz_adj != P->rz) {   // the adjoint's own tile height
+        TWI_CUDA(prepare_step(P->p.order, P->p.exact != 0, default_shape(P->rz_adj)));
+        const int TA = P->rz_adj * 4;
+        TWI_TRY(make_map(&P->ta_u2, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kBoxX,
+                         TA + 2 * HZ));
+        TWI_TRY(make_map(&P->ta_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
+                         TA));
+        TWI_TRY(make_map(&P->ta_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TA));
+    }
     if (P->tb == 2) {
         TWI_CUDA(prepare_step2(P->p.order, P->p.exact != 0, default_shape(P->rz)));
         const int rn = step2_box_rows(P->p.order, P->rz, 0), ra = step2_box_rows(P->p.order, P->rz, 1);
