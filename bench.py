@@ -313,12 +313,19 @@ def run_b200(args):
     # this grid; a launch's traffic grows with the shots it processes, so
     # other shot counts scale it by NSHOTS / 64
     traffic = None
+    traffic_source = f"ncu dram__bytes_read+write per launch at {TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}"
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                t64 = json.load(f).get(str(dom))
+                tj = json.load(f)
+            t64 = tj.get(str(dom))
             traffic = t64 * NSHOTS / TRAFFIC_SHOTS if t64 is not None else None
+            # the tile height the capture ran with, against this run's
+            rows_cap = tj.get("_rows_per_warp", {}).get(str(dom))
+            rows_now = plan.layout.adjoint_rows_per_warp if dom == 2 else plan.layout.rows_per_warp
+            if rows_cap is not None and rows_cap != rows_now:
+                traffic_source += f"; captured with {rows_cap} rows per warp, this run uses {rows_now}"
         except Exception:
             traffic = None
 
@@ -384,8 +391,7 @@ def run_b200(args):
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
-                         "traffic_source": "ncu dram__bytes_read+write per launch at "
-                                           f"{TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}",
+                         "traffic_source": traffic_source,
                          "ms_per_time_step": {names[m]: v for m, v in ms_launch.items()}},
             "plain_form": plain,
             "cpu_baseline": cpu,
