@@ -77,6 +77,25 @@ def test_plan_rejects_invalid_problem(bad):
     assert _capi.last_error()
 
 
+@pytest.mark.parametrize("rz,expect", [(0, (4, 2)), (2, (2, 2)), (4, (4, 4)), (8, (8, 8))])
+def test_rows_per_warp_per_mode(rz, expect):
+    # left open, the adjoint runs on 2-row tiles and the rest on 4; an
+    # explicit value applies to every mode
+    L = _capi.lib()
+    st, h = _create(rows_per_warp=rz)
+    assert st == _capi.TWI_OK
+    lay = _capi.Layout()
+    assert L.twi_plan_layout(h, ctypes.byref(lay)) == 0
+    assert (lay.rows_per_warp, lay.adjoint_rows_per_warp) == expect
+    L.twi_plan_destroy(h)
+
+
+def test_two_rows_per_warp_runs_one_step_per_launch():
+    st, h = _create(rows_per_warp=2, time_block=2)
+    assert st == _capi.TWI_ERR_INVALID
+    assert "rows_per_warp" in _capi.last_error()
+
+
 def test_calls_out_of_sequence_are_errors():
     L = _capi.lib()
     st, h = _create()
