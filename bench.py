@@ -377,6 +377,7 @@ def run_b200(args):
                        "shots_per_cta": plan.layout.shots_per_cta,
                        "rows_per_warp": plan.layout.rows_per_warp,
                        "adjoint_rows_per_warp": plan.layout.adjoint_rows_per_warp,
+                       "adjoint_shots_per_cta": plan.layout.adjoint_shots_per_cta,
                        "time_block": plan.layout.time_block,
                        "autotuned": bool(args.autotune),
                        "adjoint_wavefield": "boundary saving, reverse reconstruction" if args.reconstruct

@@ -127,7 +127,8 @@ typedef struct twi_problem {
     int accumulate;       /* 0: Kahan-compensated FP32 over steps and shots;
                              1: plain FP32 per shot, summed in shot order (the
                              reference's order: bit-identical gradients) */
-    int shots_per_cta;    /* shots sharing one velocity tile in a CTA; 0 = choose */
+    int shots_per_cta;    /* shots sharing one velocity tile in a CTA; 0 = choose
+                             (4, and 8 for adjoint launches) */
     int rows_per_warp;    /* 2, 4 or 8 (2: not with time_block 2); 0 = choose
                              (4, and 2 for one-step adjoint launches) */
     int use_graphs;       /* 1: capture the time loops into CUDA graphs */
@@ -162,6 +163,7 @@ typedef struct twi_layout {
     int ckpt_interval, nsegments, shots_per_cta, rows_per_warp;
     int time_block;         /* time steps per launch chosen for this plan */
     int adjoint_rows_per_warp; /* rows per warp of one-step adjoint launches */
+    int adjoint_shots_per_cta; /* shots per CTA (one Kahan group) of adjoint launches */
 } twi_layout;
 
 typedef struct twi_plan twi_plan;

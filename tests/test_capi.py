@@ -90,6 +90,20 @@ def test_rows_per_warp_per_mode(rz, expect):
     L.twi_plan_destroy(h)
 
 
+@pytest.mark.parametrize("spc,nshots,expect", [(0, 64, (4, 8)), (0, 6, (4, 6)), (0, 3, (3, 3)),
+                                              (2, 64, (2, 2)), (8, 64, (8, 8))])
+def test_shots_per_cta_per_mode(spc, nshots, expect):
+    # left open, adjoint launches take 8 shots per CTA (one Kahan pair per
+    # group) and the rest 4; an explicit value applies to every mode
+    L = _capi.lib()
+    st, h = _create(shots_per_cta=spc, nshots=nshots)
+    assert st == _capi.TWI_OK
+    lay = _capi.Layout()
+    assert L.twi_plan_layout(h, ctypes.byref(lay)) == 0
+    assert (lay.shots_per_cta, lay.adjoint_shots_per_cta) == expect
+    L.twi_plan_destroy(h)
+
+
 def test_two_rows_per_warp_runs_one_step_per_launch():
     st, h = _create(rows_per_warp=2, time_block=2)
     assert st == _capi.TWI_ERR_INVALID

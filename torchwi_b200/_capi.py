@@ -48,7 +48,8 @@ class Layout(ctypes.Structure):
                 ("dimx", ctypes.c_int), ("dimz", ctypes.c_int), ("pitch", ctypes.c_int),
                 ("ckpt_interval", ctypes.c_int), ("nsegments", ctypes.c_int),
                 ("shots_per_cta", ctypes.c_int), ("rows_per_warp", ctypes.c_int),
-                ("time_block", ctypes.c_int), ("adjoint_rows_per_warp", ctypes.c_int)]
+                ("time_block", ctypes.c_int), ("adjoint_rows_per_warp", ctypes.c_int),
+                ("adjoint_shots_per_cta", ctypes.c_int)]
 
 
 _vp = ctypes.c_void_p

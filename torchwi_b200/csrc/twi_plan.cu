@@ -144,6 +144,12 @@ constexpr int kDefaultTimeBlock = 1;
 // steps, 2 for the adjoint (whose Kahan pairs and virtual-source window halve
 // with the rows, so 5 CTAs fit an SM).  An explicit value applies to all.
 constexpr int kDefaultAdjointRows = 2;
+// Shots per CTA when the problem leaves it open: 4 for the forward-type
+// steps, 8 for the adjoint, which reads and writes its group's Kahan pairs
+// once per launch, so larger groups halve that traffic.  An explicit value
+// applies to all.
+constexpr int kDefaultShots = 4;
+constexpr int kDefaultAdjointShots = 8;
 
 LaunchShape default_shape(int rows_per_warp) {
     return LaunchShape{rows_per_warp == 8 || rows_per_warp == 2 ? rows_per_warp : 4, 4};
@@ -161,6 +167,7 @@ struct twi_plan {
     long long slot_elems = 0;
     int K = 0, nseg = 0, spc = 1, ngroups = 1, rz = 4, sps = 0;
     int rz_adj = 4;         // rows per warp of single-step adjoint launches
+    int spc_adj = 1;        // shots per CTA of adjoint launches (one Kahan pair per group)
     int tb = 1, rot = 3;   // time steps per launch (1 or 2) and rotation slots per role
     bool gradient = true, kahan = true, exa = false;
     bool recon = false;     // boundary saving + reverse reconstruction instead of checkpoints
@@ -301,6 +308,7 @@ struct twi_plan {
         a.acc = F(off_acc);
         a.acc_mode = kAccExa;
         a.acc_base = 0;
+        a.spc = spc_adj;
         a.exa = F(off_exa);
         a.iexa = reinterpret_cast<short*>(ws + off_iexa);
         for (int it = p.nt - 1; it >= 0; --it) {
@@ -337,9 +345,11 @@ struct twi_plan {
         for (int it = p.nt - 1; it >= 0; --it) {
             a.it = it;
             set_slots(a, rslot(it + 1), rslot(it), urot((it + 2) % 3), zero());
+            a.spc = spc;
             out.push_back({kModeReverse, a});
             const long long m = (long long)p.nt - 1 - it;
             set_slots(a, lam_slot(m - 2), lam_slot(m - 1), lam_slot(m), zero());
+            a.spc = spc_adj;
             out.push_back({kModeAdjoint, a});
         }
     }
@@ -366,6 +376,7 @@ struct twi_plan {
                           n == 2 ? urot((it + 2) % rot) : zero());
                 a.virt_base = it - c0;
                 a.frd = nullptr;
+                a.spc = spc;
                 out.push_back({kModeRecompute, a, n});
                 it += n;
             }
@@ -376,6 +387,7 @@ struct twi_plan {
                 set_slots(a, lam_slot(m - 2), lam_slot(m - 1), lam_slot(m),
                           n == 2 ? lam_slot(m + 1) : zero());
                 a.virt_base = it - c0;
+                a.spc = spc_adj;
                 out.push_back({kModeAdjoint, a, n});
                 it -= n;
             }
@@ -505,9 +517,10 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->K = K;
     P->nseg = (p.nt + K - 1) / K;
     int spc = p.shots_per_cta;
-    if (spc <= 0) spc = std::min(p.nshots, 4);
+    if (spc <= 0) spc = std::min(p.nshots, kDefaultShots);
     P->spc = std::min(spc, p.nshots);
-    P->ngroups = (p.nshots + P->spc - 1) / P->spc;
+    P->spc_adj = p.shots_per_cta > 0 ? P->spc : std::min(p.nshots, kDefaultAdjointShots);
+    P->ngroups = (p.nshots + P->spc_adj - 1) / P->spc_adj;   // Kahan groups of the adjoint
     if (p.time_block < 0 || p.time_block > 2) {
         delete P;
         return fail(TWI_ERR_INVALID, "time_block must be 0 (choose), 1 or 2");
@@ -570,6 +583,7 @@ int twi_plan_layout(const twi_plan* P, twi_layout* out) {
     out->shots_per_cta = P->spc;
     out->rows_per_warp = P->rz;
     out->adjoint_rows_per_warp = P->rz_adj;
+    out->adjoint_shots_per_cta = P->spc_adj;
     return TWI_OK;
 }
 
@@ -726,6 +740,7 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
         a.acc = P->F(P->off_acc);
         a.acc_comp = P->kahan ? P->F(P->off_comp) : nullptr;
         a.acc_mode = P->kahan ? kAccKahanPerGroup : kAccPlainPerShot;
+        a.spc = P->spc_adj;
     } else {
         const Slot u0 = P->urot(0), u1 = P->urot(1), u2 = P->urot(2), u3 = P->urot(P->rot - 1);
         a.prev_base = u0.base, a.cur_base = u1.base, a.next_base = u2.base, a.next2_base = u3.base;
