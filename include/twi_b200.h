@@ -222,9 +222,11 @@ int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes);
 
 /* Launch-shape autotuning (the reference has none: its CUDA path uses fixed
  * 16x16 blocks, td2d_cuda.cu).  Times every launch shape that the fields of
- * `prob` left at 0 allow -- shots per CTA 1/2/4/8 (at most nshots), rows per
- * warp 4/8, one or two time steps per launch (one for excitation amplitude)
- * -- on the current device, on a copy of the problem with nt = 8 in the
+ * `prob` left at 0 allow -- shots per CTA 0/1/2/4/8 (at most nshots), rows
+ * per warp 0/2/4/8, one or two time steps per launch (one for excitation
+ * amplitude, reverse reconstruction and 2 rows per warp; 0 = the per-mode
+ * defaults, which give the adjoint its own shape and which no single value
+ * reproduces) -- on the current device, on a copy of the problem with nt = 8 in the
  * caller's `scratch` (twi_autotune_scratch_bytes, any contents), and writes
  * *prob with the fastest shape into `tuned` and, if not NULL, its device
  * milliseconds per time step of a gradient (forward + recompute + adjoint;

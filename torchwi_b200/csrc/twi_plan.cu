@@ -784,15 +784,17 @@ int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes) {
 namespace {
 
 // The launch shapes the autotuner tries for `prob`: every combination the
-// caller left open (0) of shots per CTA {1, 2, 4, 8} (at most nshots), rows
-// per warp {2, 4, 8} and time steps per launch {1, 2} (1 for excitation
-// amplitude, reverse reconstruction and 2 rows per warp), each timed on a
-// copy of the problem with nt = 8.
+// caller left open (0) of shots per CTA {0, 1, 2, 4, 8} (at most nshots),
+// rows per warp {0, 2, 4, 8} and time steps per launch {1, 2} (1 for
+// excitation amplitude, reverse reconstruction and 2 rows per warp), each
+// timed on a copy of the problem with nt = 8.  0 keeps the per-mode defaults
+// (the adjoint's own shots per CTA and rows per warp), which no single value
+// reproduces.
 std::vector<twi_problem> tune_candidates(const twi_problem& p) {
     std::vector<twi_problem> out;
-    for (int spc : {1, 2, 4, 8}) {
+    for (int spc : {0, 1, 2, 4, 8}) {
         if (p.shots_per_cta ? spc != p.shots_per_cta : spc > std::max(1, p.nshots)) continue;
-        for (int rz : {2, 4, 8}) {
+        for (int rz : {0, 2, 4, 8}) {
             if (p.rows_per_warp && rz != p.rows_per_warp) continue;
             for (int tb : {1, 2}) {
                 if ((p.time_block && tb != p.time_block) || ((p.exa || p.reconstruct || rz == 2) && tb == 2))
