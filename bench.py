@@ -29,19 +29,35 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 NX, NZ, NT, NSHOTS = 1000, 300, 4000, 64
-ALG_BYTES = {0: 16, 1: 20, 2: 28}      # per cell-update: forward, recompute, adjoint
-MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjoint step (+gradient)"}
+# Minimal DRAM bytes per cell-update of each kernel mode as this design runs
+# it (forward; recompute + virtual-source write; adjoint + virtual-source
+# read + gradient read/write; fused backward: u^it, u^{it+1}, lambda^it,
+# lambda^{it+1}, v read, u^{it-1}, lambda^{it-1} written, gradient read/write)
+ALG_BYTES = {0: 16, 1: 20, 2: 28, 5: 36}
+# The same for the reference algorithm's steps, whatever the implementation:
+# 16 B per forward-type step (u^{n-1}, u^n, v read, u^{n+1} written), 24 B per
+# adjoint step (the same plus the gradient read and write); a backward time
+# step recomputes the forward field and takes an adjoint step: 40 B
+REF_ALG_BYTES = {0: 16, 1: 16, 2: 24, 5: 40}
+MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjoint step (+gradient)",
+              5: "fused backward step (reverse reconstruction + adjoint + gradient)"}
 TRAFFIC_SHOTS = 64                      # shots per launch of the captures in profiles/traffic.json
 
 
-def _launches_per_gradient(nt, K, time_block):
+def _launches_per_gradient(nt, K, time_block, backward="checkpoints"):
     """Kernel launches of one gradient: model padding, the forward steps, the
-    two misfit passes, per checkpoint segment its recompute and adjoint
-    steps, the gradient reduction.  Two-step launches cover pairs of steps;
-    an odd remainder runs alone."""
+    two misfit passes, the backward steps (per checkpoint segment its
+    recompute and adjoint steps; with boundary saving one fused launch per
+    step, or a rebuild and an adjoint launch), the gradient reduction.
+    Two-step launches cover pairs of steps; an odd remainder runs alone."""
     per = (lambda n: (n + 1) // 2) if time_block == 2 else (lambda n: n)
-    segments = sum(per(min(K, nt - j * K)) for j in range((nt + K - 1) // K))
-    return 1 + per(nt) + 2 + 2 * segments + 1
+    if backward == "fused":
+        back = nt
+    elif backward == "split":
+        back = 2 * nt
+    else:
+        back = 2 * sum(per(min(K, nt - j * K)) for j in range((nt + K - 1) // K))
+    return 1 + per(nt) + 2 + back + 1
 
 
 def _peak_hbm():
@@ -214,7 +230,9 @@ def run_b200(args):
     sx, sy, ry = survey.sx[mine], survey.sy[mine], survey.ry[mine]
     opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
                        shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True,
-                       time_block=args.time_block, reconstruct=args.reconstruct)
+                       time_block=args.time_block, reconstruct=args.reconstruct,
+                       split_backward=args.split_backward)
+    fused = args.reconstruct and not args.split_backward
     tuned_ms = None
     if args.autotune:   # outside the timed region
         from torchwi_b200 import autotune
@@ -230,12 +248,24 @@ def run_b200(args):
 
     misfit_buf = torch.empty((), dtype=torch.float64, device=dev)
 
-    def fwi_step(vel, obs_d):
+    # events around the forward and the backward pass of every timed step
+    # (on the launching stream, inside the timed region)
+    marks = []
+
+    def fwi_step(vel, obs_d, mark=False):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if mark else None
+        if ev:
+            ev[0].record()
         plan.set_model(vel)
         # forward with checkpoints; the receiver writes store modelled - observed
         # in the resid region and a fixed-order FP64 reduction gives the misfit
         loss = plan.forward_residual(obs_d, misfit_buf)
+        if ev:
+            ev[1].record()
         g = plan.gradient(None)
+        if ev:
+            ev[2].record()
+            marks.append(ev)
         if world > 1:
             dist.all_reduce(g)
             dist.all_reduce(loss)
@@ -271,7 +301,7 @@ def run_b200(args):
         return ms
 
     with ClockSampler(uuid) as clk:
-        ms = timed(lambda: fwi_step(vel0, obs), args.steps)
+        ms = timed(lambda: fwi_step(vel0, obs, mark=True), args.steps)
     plan.check()
     clocks = clk.summary()
     ms_step = ms / args.steps
@@ -299,33 +329,51 @@ def run_b200(args):
     h2d = vel_h.numel() * 4 + obs_h.numel() * 4
     d2h = g_h.numel() * 4 + 8
 
-    # per-kernel device time at steady state -> roofline of the dominant kernel
-    ms_launch = {m: plan.profile_step(m, repeats=args.profile_reps) for m in (0, 1, 2)}
-    dom = max(ms_launch, key=lambda m: ms_launch[m])
+    # Roofline of the dominant pass, from the events inside the timed region:
+    # the backward pass is nt launches of the fused backward kernel (or nt
+    # recompute + nt adjoint launches with checkpoints), so its time / nt is
+    # the kernel's average launch duration, graph gaps included.
+    fwd_ms = sum(e[0].elapsed_time(e[1]) for e in marks) / len(marks)
+    bwd_ms = sum(e[1].elapsed_time(e[2]) for e in marks) / len(marks)
     cells = NSHOTS * NX * NZ
-    achieved = ALG_BYTES[dom] * cells / (ms_launch[dom] / 1e3) / 1e9
     peak, peak_kind = _peak_hbm()
-    # a reconstruction plan's second pass rebuilds the field backwards
+    back_modes = (5,) if fused else (1, 2)
     names = dict(MODE_NAMES)
-    if args.reconstruct:
+    if args.reconstruct:   # a reconstruction plan's second pass rebuilds the field backwards
         names[1] = "reverse reconstruction step (+virtual source)"
+    bwd_name = names[5] if fused else f"{names[1]} + {names[2]}"
+    per_step = {"forward": fwd_ms / NT, "backward": bwd_ms / NT}
+    dom = "backward" if bwd_ms >= fwd_ms else "forward"
+    dom_modes = back_modes if dom == "backward" else (0,)
+    ref_bytes = sum(REF_ALG_BYTES[m] for m in dom_modes)
+    own_bytes = sum(ALG_BYTES[m] for m in dom_modes)
+    achieved = ref_bytes * cells / (per_step[dom] / 1e3) / 1e9
+    achieved_own = own_bytes * cells / (per_step[dom] / 1e3) / 1e9
+    # the same kernels launched alone, back to back (after the timed region)
+    iso_modes = (0,) + back_modes
+    ms_launch = {m: plan.profile_step(m, repeats=args.profile_reps) for m in iso_modes}
     # DRAM bytes per launch from one ncu capture of each mode at 64 shots on
-    # this grid; a launch's traffic grows with the shots it processes, so
-    # other shot counts scale it by NSHOTS / 64
+    # this grid at the shipped launch shape; a launch's traffic grows with the
+    # shots it processes, so other shot counts scale it by NSHOTS / 64
     traffic = None
-    traffic_source = f"ncu dram__bytes_read+write per launch at {TRAFFIC_SHOTS} shots, scaled by {NSHOTS}/{TRAFFIC_SHOTS}"
+    traffic_source = (f"ncu dram__bytes_read+write per launch at {TRAFFIC_SHOTS} shots, scaled by "
+                      f"{NSHOTS}/{TRAFFIC_SHOTS}, summed over the pass's kernels per time step")
     tpath = os.path.join(REPO, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
                 tj = json.load(f)
-            t64 = tj.get(str(dom))
-            traffic = t64 * NSHOTS / TRAFFIC_SHOTS if t64 is not None else None
-            # the tile height the capture ran with, against this run's
-            rows_cap = tj.get("_rows_per_warp", {}).get(str(dom))
-            rows_now = plan.layout.adjoint_rows_per_warp if dom == 2 else plan.layout.rows_per_warp
-            if rows_cap is not None and rows_cap != rows_now:
-                traffic_source += f"; captured with {rows_cap} rows per warp, this run uses {rows_now}"
+            parts = [tj.get(str(m)) for m in dom_modes]
+            if all(t is not None for t in parts):
+                traffic = sum(parts) * NSHOTS / TRAFFIC_SHOTS
+            # the launch shape the capture ran with, against this run's
+            for m in dom_modes:
+                cap = tj.get("_shape", {}).get(str(m))
+                adj = m in (2, 5)
+                now = [plan.layout.adjoint_rows_per_warp if adj else plan.layout.rows_per_warp,
+                       plan.layout.adjoint_shots_per_cta if adj else plan.layout.shots_per_cta]
+                if cap is not None and list(cap) != now:
+                    traffic_source += f"; mode {m} captured at (rows per warp, shots per CTA) {cap}, this run {now}"
         except Exception:
             traffic = None
 
@@ -333,7 +381,8 @@ def run_b200(args):
     plain = None
     if args.plain_shots > 0 and rank == 0:
         popts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
-                            shots_per_cta=1, use_graphs=False)
+                            shots_per_cta=1, use_graphs=False, reconstruct=args.reconstruct,
+                            split_backward=args.split_backward)
         p1 = ShotPlan(NX, NZ, survey.h, survey.dt, NT, 4, nshots=1, options=popts, device=dev)
         p1.set_wavelet(torch.from_numpy(survey.w))
 
@@ -361,8 +410,9 @@ def run_b200(args):
     if world > 1:
         dist.barrier()
     if rank == 0:
-        launches = args.steps * _launches_per_gradient(NT, plan.layout.ckpt_interval,
-                                                       plan.layout.time_block)
+        launches = args.steps * _launches_per_gradient(
+            NT, plan.layout.ckpt_interval, plan.layout.time_block,
+            "fused" if fused else "split" if args.reconstruct else "checkpoints")
         line = {
             "metric": "shot-gradients/s", "value": value, "unit": "shot-gradients/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -380,7 +430,9 @@ def run_b200(args):
                        "adjoint_shots_per_cta": plan.layout.adjoint_shots_per_cta,
                        "time_block": plan.layout.time_block,
                        "autotuned": bool(args.autotune),
-                       "adjoint_wavefield": "boundary saving, reverse reconstruction" if args.reconstruct
+                       "adjoint_wavefield": ("boundary saving, reverse reconstruction, "
+                                             + ("rebuild and adjoint launches" if args.split_backward
+                                                else "fused backward launch")) if args.reconstruct
                                             else f"checkpoints every {plan.layout.ckpt_interval} steps",
                        "l2": "inputs larger than L2 (workspace %.1f GB)" % (plan.workspace.numel() / 1e9)},
             "gcell_per_s": gcell,
@@ -388,12 +440,21 @@ def run_b200(args):
             "e2e": {"value": total_shots / (ms_e2e / 1e3), "unit": "shot-gradients/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved,
-                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "roofline": {"bound": "hbm", "kernel": bwd_name if dom == "backward" else names[0],
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                         "alg_bytes_per_cell": ALG_BYTES[dom], "traffic": traffic,
-                         "traffic_source": traffic_source,
-                         "ms_per_time_step": {names[m]: v for m, v in ms_launch.items()}},
+                         "alg_bytes_per_cell": ref_bytes,
+                         "alg_bytes_basis": "reference algorithm: 16 B per forward-type step, 24 B per "
+                                            "adjoint step, per cell-update; one launch = "
+                                            f"{cells} cell-updates",
+                         "own_alg_bytes_per_cell": own_bytes,
+                         "frac_own_bytes": achieved_own / peak,
+                         "traffic": traffic, "traffic_source": traffic_source,
+                         "ms_per_time_step": {"forward pass": per_step["forward"],
+                                              "backward pass": per_step["backward"],
+                                              "source": "CUDA events around each pass of every timed step"},
+                         "isolated_launch_ms": {names[m]: v for m, v in ms_launch.items()},
+                         "whole_gradient_frac": 56.0 * cells * NT / (ms_step / 1e3) / 1e9 / peak},
             "plain_form": plain,
             "cpu_baseline": cpu,
         }
@@ -549,6 +610,8 @@ def main():
     ap.add_argument("--autotune", action="store_true", help="time the launch shapes first and use the fastest")
     ap.add_argument("--reconstruct", action="store_true",
                     help="boundary saving + reverse reconstruction instead of checkpoints")
+    ap.add_argument("--split-backward", action="store_true",
+                    help="with --reconstruct: rebuild and adjoint as two launches per step")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--profile-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")

@@ -86,11 +86,12 @@ int twi_fdm_forward_only(float* frd, float* u1, float* u2, float* u3, const floa
  * scratch is a file-scope device array of 32 MiB reserved on every GPU that
  * loads the library: grids need
  *   5 * roundup(dimx,128) * dimy * 4 + nt * 4 bytes (+ < 2 KiB)
- * to fit, larger ones are rejected with TWI_ERR_INVALID.  The first call on
- * a device looks up the scratch address (cudaGetSymbolAddress) and should
- * come before any stream capture.  All calls share the scratch: calls whose
- * work overlaps on the GPU race, so issue them on one stream or synchronise
- * between them.  Synchronises `stream` before returning. */
+ * to fit, larger ones are rejected with TWI_ERR_INVALID.  Every call looks
+ * up the scratch address on the current device (cudaGetSymbolAddress)
+ * before any work, so the address stays valid across device resets.  All
+ * calls share the scratch: calls whose work overlaps on the GPU race, so
+ * issue them on one stream or synchronise between them.  Synchronises
+ * `stream` before returning. */
 int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const float* w, int order,
                                  int dimx, int dimy, int nt, float h, float dt, float sx,
                                  float sy, float ry, void* stream);
@@ -146,9 +147,14 @@ typedef struct twi_problem {
                              gradient pass rebuilds the wavefield backwards from the
                              last two levels; (nt+1) * nshots * boundary cells floats
                              instead of the checkpoint and virtual-source slots.
-                             Gradients agree with the reference within its FP32
-                             tolerance, not bit for bit.  One step per launch;
-                             plan-level calls only */
+                             Each backward step is one fused launch: rebuild, virtual
+                             source (in registers), adjoint step and gradient term.
+                             2: the same with the rebuild and the adjoint step as two
+                             launches per step and the virtual source passed through
+                             one slot per shot.  Gradients agree with the reference
+                             within its FP32 tolerance, not bit for bit (1 and 2 give
+                             the same bits).  One step per launch; plan-level calls
+                             only */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */
@@ -202,8 +208,9 @@ int twi_plan_check(twi_plan* plan, void* stream);
 /* Measurement hook (no counterpart in the reference): launch `repeats`
  * steady-state time steps of one kernel mode (0 forward, 1 recompute with
  * virtual-source output -- the reverse reconstruction for plans with
- * `reconstruct` --, 2 adjoint with gradient accumulation; 10, 11, 12 the
- * two-step launches of the same modes for plans with time_block 2) for all
+ * `reconstruct` --, 2 adjoint with gradient accumulation, 5 the fused
+ * backward step of plans with reconstruct = 1; 10, 11, 12 the
+ * two-step launches of modes 0-2 for plans with time_block 2) for all
  * shots and return the mean device time per launch in *ms_per_launch (CUDA
  * events on `stream`).  Overwrites rotating wavefield slots and the gradient
  * accumulators, never the checkpoints; call after twi_forward. */

@@ -68,6 +68,26 @@ def test_reconstructed_config2_shot_full_size():
     assert err <= GRAD_TOL
 
 
+@pytest.mark.parametrize("order", [2, 4, 8])
+@pytest.mark.parametrize("accumulate", ["plain", "kahan"])
+@pytest.mark.parametrize("shape", [(80, 40, 300, 3, 0), (37, 23, 200, 11, 4), (130, 41, 120, 9, 2)])
+def test_fused_backward_equals_split_launches(order, accumulate, shape):
+    """One fused launch per backward step (the virtual source in registers)
+    gives the same bits as the rebuild and adjoint launches with the virtual
+    source passed through memory."""
+    nx, nz, nt, nshots, rz = shape
+    s = synthetic.small_case(nx=nx, nz=nz, nt=nt, order=order, nshots=nshots, seed=nx + nshots)
+    grads = []
+    for split in (False, True):
+        p = _plan(s, accumulate=accumulate, reconstruct=True, split_backward=split, rows_per_warp=rz)
+        p.set_model(torch.from_numpy(s.vel_start).cuda())
+        f = p.forward(save_checkpoints=True)
+        grads.append(p.gradient(0.5 * f).cpu().numpy())
+        p.check()
+    assert bits_equal(grads[0], grads[1])
+    assert np.abs(grads[0]).max() > 0
+
+
 def test_reconstruction_plans_stay_out_of_batches():
     s = synthetic.small_case(nx=40, nz=20, nt=50, nshots=2)
     p = _plan(s, reconstruct=True)

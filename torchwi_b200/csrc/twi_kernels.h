@@ -19,6 +19,9 @@ enum StepMode : int {
     kModeReverse = 4,     // u^{n-1} from u^n and u^{n+1} (the forward step run
                           // backwards, source removed); pad cells restored
                           // from the boundary buffer; virtual source written
+    kModeBackward = 5,    // kModeReverse and kModeAdjoint of the same step in
+                          // one pass (twi_backward.cu): the virtual source
+                          // stays in registers
 };
 
 // Gradient accumulator layout used by kModeAdjoint.
@@ -81,6 +84,11 @@ struct StepArgs {
     int acc_mode;
     int acc_base;               // slot of group 0 / shot 0
     int* err;                   // device error word (bit 0: TMA wait timeout)
+    // kModeBackward: the adjoint field's slots (prev/cur/next above hold
+    // u^{it+1}, u^it and the rebuilt u^{it-1})
+    int lprev_base, lprev_stride;
+    int lcur_base, lcur_stride;
+    int lnext_base, lnext_stride;
 };
 
 // The part of a time step's arguments that changes from step to step.
@@ -170,6 +178,17 @@ cudaError_t launch_step2(int order, bool exact, StepMode mode, LaunchShape shape
                          const CUtensorMap& tm_un, const CUtensorMap& tm_um, const CUtensorMap& tm_v,
                          const StepArgs& a, cudaStream_t stream);
 cudaError_t prepare_step2(int order, bool exact, LaunchShape shape);
+
+// Fused backward step of boundary-saving plans (twi_backward.cu): rebuild
+// u^{it-1} (kModeReverse), step lambda (kModeAdjoint) and accumulate the
+// gradient with the virtual source held in registers.  Same tensor maps as
+// launch_step (tm_c: (136, TZ + order) box, tm_p and tm_vel: (128, TZ));
+// rows_per_warp 2 or 4.
+int backward_ctas(int order, int rows_per_warp, const StepArgs& a, int* nbc);
+cudaError_t launch_backward(int order, bool exact, LaunchShape shape, const CUtensorMap& tm_c,
+                            const CUtensorMap& tm_p, const CUtensorMap& tm_vel, const StepArgs& a,
+                            cudaStream_t stream);
+cudaError_t prepare_backward(int order, bool exact, LaunchShape shape);
 
 // Store n host integers into device memory through kernel parameters
 // (chunks of 2048), ordered on `stream` without a host synchronisation.

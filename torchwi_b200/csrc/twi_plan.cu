@@ -84,6 +84,10 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
+}  // namespace
+
+namespace twi {
+
 // Tensor map over `nslots` slots of [dimz][pitch] floats (x extent dimx, so
 // reads past the last column return zeros); nslots == 0 gives a 2-D map.
 int make_map(CUtensorMap* tm, const void* base, int dimx, int dimz, long long nslots, int pitch,
@@ -103,12 +107,6 @@ int make_map(CUtensorMap* tm, const void* base, int dimx, int dimz, long long ns
         return fail(TWI_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
     return TWI_OK;
 }
-
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-struct Slot {
-    int base, stride;
-};
 
 // Cell lookup exactly as the reference: FP32 division, truncation toward 0
 // (propagator_cpu.cpp:44-48).
@@ -137,6 +135,16 @@ int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, in
     *rec_r = iry + ne;
     return TWI_OK;
 }
+
+}  // namespace twi
+
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Slot {
+    int base, stride;
+};
 
 // Time steps per launch when the problem leaves it open.
 constexpr int kDefaultTimeBlock = 1;
@@ -171,6 +179,7 @@ struct twi_plan {
     int tb = 1, rot = 3;   // time steps per launch (1 or 2) and rotation slots per role
     bool gradient = true, kahan = true, exa = false;
     bool recon = false;     // boundary saving + reverse reconstruction instead of checkpoints
+    bool fused_back = false;   // recon: one fused backward launch per step (else reverse + adjoint)
     int nb = 0;             // boundary (Keys) cells per shot and time level
     long long nslots = 0, nvirt = 0, nacc = 0;
     // workspace regions (byte offsets)
@@ -257,7 +266,14 @@ struct twi_plan {
     }
 
     int launch(StepMode mode, const StepArgs& a, cudaStream_t st, int nsteps = 1) const {
-        const bool adj = nsteps == 1 && mode == kModeAdjoint && rz_adj != rz;
+        const bool adj = nsteps == 1 && (mode == kModeAdjoint || mode == kModeBackward) && rz_adj != rz;
+        if (mode == kModeBackward) {
+            cudaError_t e = adj ? launch_backward(p.order, p.exact != 0, default_shape(rz_adj), ta_u2, ta_u1, ta_vel, a, st)
+                                : launch_backward(p.order, p.exact != 0, default_shape(rz), tm_u2, tm_u1, tm_vel, a, st);
+            if (e != cudaSuccess)
+                return fail(TWI_ERR_CUDA, std::string("backward launch: ") + cudaGetErrorString(e));
+            return TWI_OK;
+        }
         cudaError_t e = nsteps == 2
             ? launch_step2(p.order, p.exact != 0, mode, default_shape(rz), tm2_un, tm2_um, tm2_v, a, st)
             : adj ? launch_step(p.order, p.exact != 0, mode, default_shape(rz_adj), ta_u2, ta_u1, ta_vel, a, st)
@@ -274,6 +290,12 @@ struct twi_plan {
         a.cur_base = cu.base, a.cur_stride = cu.stride;
         a.next_base = nx.base, a.next_stride = nx.stride;
         a.next2_base = nx2.base, a.next2_stride = nx2.stride;
+    }
+
+    static void set_lam_slots(StepArgs& a, Slot pv, Slot cu, Slot nx) {
+        a.lprev_base = pv.base, a.lprev_stride = pv.stride;
+        a.lcur_base = cu.base, a.lcur_stride = cu.stride;
+        a.lnext_base = nx.base, a.lnext_stride = nx.stride;
     }
 
     // The forward pass as a list of launches: pairs of time steps when the
@@ -342,6 +364,17 @@ struct twi_plan {
         a.bnd = F(off_bnd);
         a.bnd_cells = nb;
         auto rslot = [&](long long k) { return k <= 0 ? zero() : urot((int)(k % 3)); };
+        if (fused_back) {   // one launch per step; the virtual source stays in registers
+            a.spc = spc_adj;
+            for (int it = p.nt - 1; it >= 0; --it) {
+                const long long m = (long long)p.nt - 1 - it;
+                a.it = it;
+                set_slots(a, rslot(it + 1), rslot(it), urot((it + 2) % 3), zero());
+                set_lam_slots(a, lam_slot(m - 2), lam_slot(m - 1), lam_slot(m));
+                out.push_back({kModeBackward, a});
+            }
+            return;
+        }
         for (int it = p.nt - 1; it >= 0; --it) {
             a.it = it;
             set_slots(a, rslot(it + 1), rslot(it), urot((it + 2) % 3), zero());
@@ -525,11 +558,17 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
         delete P;
         return fail(TWI_ERR_INVALID, "time_block must be 0 (choose), 1 or 2");
     }
+    if (p.reconstruct < 0 || p.reconstruct > 2) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "reconstruct must be 0, 1 (fused backward) or 2 (reverse and adjoint launches)");
+    }
     P->recon = p.reconstruct != 0 && P->gradient && !P->exa;
+    P->fused_back = P->recon && p.reconstruct == 1;
     if (P->recon && p.time_block == 2) {
         delete P;
         return fail(TWI_ERR_INVALID, "reverse reconstruction runs one time step per launch");
     }
+    if (P->fused_back && P->rz_adj == 8) P->rz_adj = 4;   // the fused kernel has 2- and 4-row tiles
     P->tb = P->exa || P->recon ? 1 : p.time_block == 0 ? kDefaultTimeBlock : p.time_block;
     P->rot = P->tb == 2 ? 4 : 3;
     if (P->recon) {   // no checkpoints: one segment, one virtual-source slot per shot
@@ -539,7 +578,8 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->nb = 2 * P->ne * (P->dimz - 2 * P->ne) + P->ne * P->dimx;
     P->sps = P->gradient ? 2 * P->rot + (P->exa || P->recon ? 0 : 2 * (P->nseg - 1)) : P->rot;
     P->nslots = 1 + (long long)p.nshots * P->sps;
-    P->nvirt = P->gradient && !P->exa ? (long long)p.nshots * (P->recon ? 1 : K) : 0;
+    // the fused backward keeps the virtual source in registers: no slots
+    P->nvirt = P->gradient && !P->exa && !P->fused_back ? (long long)p.nshots * (P->recon ? 1 : K) : 0;
     P->nacc = P->gradient ? (P->kahan ? P->ngroups : p.nshots) : 0;
 
     // workspace layout
@@ -604,6 +644,7 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
     TWI_TRY(make_map(&P->tm_u1, P->F(P->off_fields), P->dimx, P->dimz, P->nslots, P->pitch, kTileX,
                      TZ));
     TWI_TRY(make_map(&P->tm_vel, P->F(P->off_vpad), P->dimx, P->dimz, 0, P->pitch, kTileX, TZ));
+    if (P->fused_back) TWI_CUDA(prepare_backward(P->p.order, P->p.exact != 0, default_shape(P->rz_adj)));
     if (P->gradient && P->rz_adj != P->rz) {   // the adjoint's own tile height
         TWI_CUDA(prepare_step(P->p.order, P->p.exact != 0, default_shape(P->rz_adj)));
         const int TA = P->rz_adj * 4;
@@ -723,8 +764,12 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
     if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
     const int nsteps = mode >= 10 ? 2 : 1;
     mode = mode >= 10 ? mode - 10 : mode;
-    if (!ms_per_launch || repeats < 1 || mode < 0 || mode > 2)
-        return fail(TWI_ERR_INVALID, "mode must be 0, 1, 2 (one step) or 10, 11, 12 (two steps) and repeats >= 1");
+    if (!ms_per_launch || repeats < 1 || mode < 0 || (mode > 2 && mode != 5) || (nsteps == 2 && mode == 5))
+        return fail(TWI_ERR_INVALID, "mode must be 0, 1, 2, 5 (one step) or 10, 11, 12 (two steps) and repeats >= 1");
+    if (mode == 5 && !P->fused_back)
+        return fail(TWI_ERR_INVALID, "mode 5 (fused backward) needs a plan with reconstruct = 1");
+    if ((mode == 1 || mode == 2) && (P->fused_back || !P->gradient || P->exa))
+        return fail(TWI_ERR_INVALID, "modes 1 and 2 need a gradient plan with checkpoints or reconstruct = 2");
     if (nsteps == 2 && P->tb != 2) return fail(TWI_ERR_INVALID, "two-step launches need a plan with time_block 2");
     if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -732,7 +777,19 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
     const int it = P->p.nt / 2;
     a.it = it;
     StepMode m = static_cast<StepMode>(mode);
-    if (m == kModeAdjoint) {
+    if (m == kModeBackward) {
+        const Slot u0 = P->urot(0), u1 = P->urot(1), u2 = P->urot(2);
+        const Slot l0 = P->lrot(0), l1 = P->lrot(1), l2 = P->lrot(2);
+        twi_plan::set_slots(a, u0, u1, u2, P->zero());
+        twi_plan::set_lam_slots(a, l0, l1, l2);
+        a.resid = P->F(P->off_frd);
+        a.acc = P->F(P->off_acc);
+        a.acc_comp = P->kahan ? P->F(P->off_comp) : nullptr;
+        a.acc_mode = P->kahan ? kAccKahanPerGroup : kAccPlainPerShot;
+        a.bnd = P->F(P->off_bnd);
+        a.bnd_cells = P->nb;
+        a.spc = P->spc_adj;
+    } else if (m == kModeAdjoint) {
         const Slot l0 = P->lrot(0), l1 = P->lrot(1), l2 = P->lrot(2), l3 = P->lrot(P->rot - 1);
         a.prev_base = l0.base, a.cur_base = l1.base, a.next_base = l2.base, a.next2_base = l3.base;
         a.virt_in = P->F(P->off_virt);
@@ -751,7 +808,7 @@ int twi_plan_profile(twi_plan* P, int mode, int repeats, float* ms_per_launch, v
             a.bnd_cells = P->nb;
         }
     }
-    a.prev_stride = a.cur_stride = a.next_stride = a.next2_stride = P->sps;
+    if (m != kModeBackward) a.prev_stride = a.cur_stride = a.next_stride = a.next2_stride = P->sps;
     a.virt_stride = P->recon ? 1 : P->K;
     a.virt_base = m == kModeAdjoint && !P->recon ? 1 : 0;   // two-step adjoint reads slots 1 and 0
     cudaEvent_t e0, e1;
@@ -852,8 +909,14 @@ int twi_autotune(const twi_problem* prob, void* scratch, size_t scratch_bytes, v
             s = fail(TWI_ERR_CUDA, "model upload failed");
         if (s == TWI_OK) s = twi_plan_set_model(P, stream);
         float total = 0.f;
-        const int modes = P->gradient ? 3 : 1;
-        for (int m = 0; m < modes && s == TWI_OK; ++m) {
+        // forward, recompute, adjoint; forward and the fused backward for
+        // boundary-saving plans; the forward step alone for forward-only and
+        // excitation-amplitude plans
+        std::vector<int> modes{0};
+        if (P->fused_back) modes.push_back(5);
+        else if (P->gradient && !P->exa) modes.insert(modes.end(), {1, 2});
+        for (size_t mi = 0; mi < modes.size() && s == TWI_OK; ++mi) {
+            const int m = modes[mi];
             const int mode = P->tb == 2 ? 10 + m : m;
             float ms = 0.f;
             s = twi_plan_profile(P, mode, 2, &ms, stream);           // warm-up

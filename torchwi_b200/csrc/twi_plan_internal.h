@@ -2,6 +2,7 @@
 // the library (not part of the C ABI).
 #pragma once
 
+#include <string>
 #include <vector>
 
 #include "twi_b200.h"
@@ -17,6 +18,22 @@ struct TwiStep {
     StepArgs a;
     int nsteps = 1;
 };
+
+// Shared by the plan and the allocation-free entry point (twi_plan.cu); each
+// reports its failure through twi_last_error.
+// Tensor map over `nslots` slots of [dimz][pitch] floats (x extent dimx);
+// nslots == 0 gives a 2-D map.
+int make_map(CUtensorMap* tm, const void* base, int dimx, int dimz, long long nslots, int pitch,
+             int box_x, int box_z);
+// order must be 2, 4 or 8.
+int check_order(int order);
+// The reference's cell lookup (int)(coord/h) in FP32 (propagator_cpu.cpp:44-48).
+int cell_of(float coord, float h);
+// Padded source row/column and receiver row of one shot; the shot must lie
+// inside the model and the receiver row inside the grid.
+int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, int dimz, int* src_r,
+               int* src_c, int* rec_r);
+void set_last_error(const std::string& msg);
 
 }  // namespace twi
 

@@ -24,11 +24,10 @@
 #include "twi_cell.cuh"
 #include "twi_kernels.h"
 #include "twi_ptx.cuh"
+#include "twi_tile.cuh"
 
 namespace twi {
 namespace {
-
-constexpr int round32(int n) { return (n + 31) / 32 * 32; }
 
 // CTAs per SM the launch bounds ask for: 2 rows per warp -> 5, 4 -> 4, 8 -> 2
 // (the 8-row tiles are held to 2 by shared memory)
@@ -53,27 +52,6 @@ struct Smem {
     static constexpr uint32_t V_TX = TZ * kTileX * 4;
 };
 
-__device__ __forceinline__ float comp(const float4& v, int m) {
-    return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ void set_comp(float4& v, int m, float x) {
-    if (m == 0) v.x = x;
-    else if (m == 1) v.y = x;
-    else if (m == 2) v.z = x;
-    else v.w = x;
-}
-__device__ __forceinline__ float4 ld4(const float* p) {
-    return *reinterpret_cast<const float4*>(p);
-}
-
-// Number of Keys boundary cells of one shot: the left and right ne columns of
-// rows [ne, dimz-ne) and all columns of the bottom ne rows
-// (td2d_cpu.cpp:116-145).
-__host__ __device__ inline int boundary_cells(int order, int dimx, int dimz) {
-    const int ne = order / 2;
-    return 2 * ne * (dimz - 2 * ne) + ne * dimx;
-}
-
 // One boundary CTA: a strided share of the Keys cells of one shot group,
 // one thread per cell, for every shot of the group.  Neighbours come
 // straight from the slots (L2); the interior CTAs never write these cells.
@@ -82,25 +60,11 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
     constexpr int NE = ORDER / 2;
     const int grp = b / nbc, part = b - grp * nbc;
     const int s0 = grp * a.spc, s1 = min(s0 + a.spc, a.nshots);
-    const int side_rows = a.dimz - 2 * NE;
-    const int n_side = 2 * NE * side_rows;
-    const int nb = n_side + NE * a.dimx;
+    const int nb = boundary_cells(ORDER, a.dimx, a.dimz);
     for (int idx = part * blockDim.x + threadIdx.x; idx < nb; idx += nbc * blockDim.x) {
         int r, c;
         long long db;   // offset to the first cell inwards
-        if (idx < n_side) {
-            const int side = idx / (NE * side_rows);
-            const int rem = idx - side * NE * side_rows;
-            r = NE + rem / NE;
-            const int k = rem - (rem / NE) * NE;
-            c = side == 0 ? k : a.dimx - NE + k;
-            db = side == 0 ? 1 : -1;
-        } else {
-            const int j = idx - n_side;
-            r = a.dimz - NE + j / a.dimx;
-            c = j - (j / a.dimx) * a.dimx;
-            db = -(long long)a.pitch;
-        }
+        boundary_cell_at<NE>(idx, a.dimx, a.dimz, a.pitch, r, c, db);
         const long long cell = (long long)r * a.pitch + c;
         const float v = a.vel[cell];
         const float q = (MODE == kModeRecompute || MODE == kModeExaForward || MODE == kModeReverse)

@@ -33,6 +33,7 @@
 #include "twi_cell.cuh"
 #include "twi_kernels.h"
 #include "twi_ptx.cuh"
+#include "twi_tile.cuh"
 
 namespace twi {
 namespace {
@@ -40,8 +41,6 @@ namespace {
 constexpr int kOutX = kTile2X;          // output columns per tile
 constexpr int kRegX = 128;              // step-A columns: output + 4 each side
 constexpr int kUnX = kRegX + 8;         // staged u^n columns: step A + 4 each side
-
-constexpr int round32(int n) { return (n + 31) / 32 * 32; }
 
 template <int ORDER, int RZ, int WZ>
 struct Smem2 {
@@ -65,16 +64,6 @@ struct Smem2 {
     static constexpr uint32_t V_TX = RA * kRegX * 4;
 };
 
-__device__ __forceinline__ float comp(const float4& v, int m) {
-    return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
-}
-__device__ __forceinline__ void set_comp(float4& v, int m, float x) {
-    if (m == 0) v.x = x;
-    else if (m == 1) v.y = x;
-    else if (m == 2) v.z = x;
-    else v.w = x;
-}
-__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 
 // One Keys cell from shared memory: `uo` points at u^n of the cell, `so` is
 // the offset to the next cell inwards in that buffer; `um` / `sm` the same

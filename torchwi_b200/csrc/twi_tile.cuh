@@ -1,0 +1,57 @@
+// twi_tile.cuh -- small device helpers shared by the tile kernels
+// (twi_step.cu, twi_backward.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "twi_kernels.h"
+
+namespace twi {
+
+constexpr int round32(int n) { return (n + 31) / 32 * 32; }
+
+__device__ __forceinline__ float comp(const float4& v, int m) {
+    return m == 0 ? v.x : m == 1 ? v.y : m == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ void set_comp(float4& v, int m, float x) {
+    if (m == 0) v.x = x;
+    else if (m == 1) v.y = x;
+    else if (m == 2) v.z = x;
+    else v.w = x;
+}
+__device__ __forceinline__ float4 ld4(const float* p) {
+    return *reinterpret_cast<const float4*>(p);
+}
+
+// Number of Keys boundary cells of one shot: the left and right ne columns of
+// rows [ne, dimz-ne) and all columns of the bottom ne rows
+// (td2d_cpu.cpp:116-145).
+__host__ __device__ inline int boundary_cells(int order, int dimx, int dimz) {
+    const int ne = order / 2;
+    return 2 * ne * (dimz - 2 * ne) + ne * dimx;
+}
+
+// Row, column and inward step (offset to the next cell towards the interior)
+// of boundary cell `idx` in the boundary CTAs' order: left columns, right
+// columns (row by row, ne cells each), then the bottom rows.
+template <int NE>
+__device__ __forceinline__ void boundary_cell_at(int idx, int dimx, int dimz, int pitch, int& r,
+                                                 int& c, long long& db) {
+    const int side_rows = dimz - 2 * NE;
+    const int n_side = 2 * NE * side_rows;
+    if (idx < n_side) {
+        const int side = idx / (NE * side_rows);
+        const int rem = idx - side * NE * side_rows;
+        r = NE + rem / NE;
+        const int k = rem - (rem / NE) * NE;
+        c = side == 0 ? k : dimx - NE + k;
+        db = side == 0 ? 1 : -1;
+    } else {
+        const int j = idx - n_side;
+        r = dimz - NE + j / dimx;
+        c = j - (j / dimx) * dimx;
+        db = -(long long)pitch;
+    }
+}
+
+}  // namespace twi

@@ -45,7 +45,11 @@ class PlanOptions:
                  the absorbing-boundary cells of every step and the gradient
                  pass rebuilds the wavefield backwards in time (much less
                  memory; gradients within FP32 tolerance of the reference,
-                 not bit-identical).
+                 not bit-identical).  Each backward step is one fused launch
+                 (rebuild, virtual source, adjoint step, gradient term).
+    split_backward: with reconstruct, run the rebuild and the adjoint step
+                 as two launches per step with the virtual source passed
+                 through memory (the same bits; kept for comparison).
     """
 
     exact: bool = True
@@ -58,6 +62,7 @@ class PlanOptions:
     exa: bool = False
     time_block: int = 0
     reconstruct: bool = False
+    split_backward: bool = False
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -88,7 +93,7 @@ def autotune(nx, nz, nshots, order=4, h=10.0, dt=1e-3, options: PlanOptions | No
     o = options or PlanOptions()
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     key = (dev.index, nx, nz, nshots, order, o.exact, o.accumulate, o.forward_only, o.exa,
-           o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct)
+           o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct, o.split_backward)
     if key in _TUNED:
         return _TUNED[key]
     import dataclasses
@@ -133,7 +138,8 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    shots_per_cta=int(o.shots_per_cta), rows_per_warp=int(o.rows_per_warp),
                    use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
                    forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)),
-                   time_block=int(o.time_block), reconstruct=int(bool(o.reconstruct)))
+                   time_block=int(o.time_block),
+                   reconstruct=(2 if o.split_backward else 1) if o.reconstruct else 0)
 
 
 class ShotPlan:
@@ -243,16 +249,17 @@ class ShotPlan:
 
     def profile_step(self, mode: int, repeats: int = 20) -> float:
         """Mean device milliseconds per TIME STEP of one kernel mode (0
-        forward, 1 recompute, 2 adjoint) as this plan launches it: a two-step
-        launch's time is halved."""
+        forward, 1 recompute, 2 adjoint, 5 the fused backward step of a
+        boundary-saving plan) as this plan launches it: a two-step launch's
+        time is halved."""
         if self.layout.time_block == 2:
             return self.profile(10 + mode, repeats) / 2
         return self.profile(mode, repeats)
 
     def profile(self, mode: int, repeats: int = 20) -> float:
         """Mean device milliseconds per launch of one kernel mode (0 forward,
-        1 recompute, 2 adjoint; 10, 11, 12 the two-step launches of a plan
-        with time_block 2) at steady state, all shots."""
+        1 recompute, 2 adjoint, 5 fused backward; 10, 11, 12 the two-step
+        launches of a plan with time_block 2) at steady state, all shots."""
         ms = ctypes.c_float()
         with torch.cuda.device(self.device):
             check(self._lib.twi_plan_profile(self._h, int(mode), int(repeats), ctypes.byref(ms),
