@@ -91,3 +91,4 @@ def test_no_alloc_rejects_oversized_grid():
                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert st == _capi.TWI_ERR_INVALID
     assert "too large" in _capi.last_error()
+

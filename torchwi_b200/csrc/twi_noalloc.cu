@@ -11,9 +11,10 @@
 // caller passes only inputs and outputs.
 //
 // Rules that follow from the shared array:
-//   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture;
+//   * every call looks up the array's device address with
+//     cudaGetSymbolAddress on the current device before it does anything
+//     else, so the address is never stale (after a device reset the module
+//     may load again at another address);
 //   * every call reuses the same array and leaves its contents behind: the
 //     call clears what must start at zero (the zero wavefield slot and the
 //     error word) itself;
@@ -24,15 +25,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "twi_b200.h"
 #include "twi_kernels.h"
-
-namespace twi {
-void set_last_error(const std::string& msg);   // twi_plan.cu
-}
+#include "twi_plan_internal.h"
 
 namespace {
 
@@ -45,54 +42,14 @@ int nofail(int code, const std::string& msg) {
     return code;
 }
 
-// Device address of g_noalloc_scratch on the current device (looked up once
-// per device; host code must not use the symbol's name as an address).
+// Device address of g_noalloc_scratch on the current device, looked up on
+// every call (host code must not use the symbol's name as an address).
 int scratch_address(unsigned char** out) {
-    static std::mutex mu;
-    static unsigned char* addr[64] = {};
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return nofail(TWI_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= 64) return nofail(TWI_ERR_CUDA, "device index out of range");
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return nofail(TWI_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") +
-                                            cudaGetErrorString(e));
-        addr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = addr[dev];
-    return TWI_OK;
-}
-
-using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                              const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                              const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                              CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-int encode(CUtensorMap* tm, void* base, int dimx, int dimz, int nslots, int pitch, int box_x,
-           int box_z) {
-    static EncodeFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-                cudaSuccess && q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeFn>(p);
-    });
-    if (!fn) return nofail(TWI_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
-    const cuuint32_t rank = nslots > 0 ? 3 : 2;
-    cuuint64_t dims[3] = {(cuuint64_t)dimx, (cuuint64_t)dimz, (cuuint64_t)(nslots > 0 ? nslots : 1)};
-    cuuint64_t strides[2] = {(cuuint64_t)pitch * 4, (cuuint64_t)pitch * dimz * 4};
-    cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_z, 1};
-    cuuint32_t estr[3] = {1, 1, 1};
-    if (fn(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, base, dims, strides, box, estr,
-           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return nofail(TWI_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return nofail(TWI_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+    *out = static_cast<unsigned char*>(p);
     return TWI_OK;
 }
 
@@ -106,23 +63,30 @@ extern "C" int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const 
                                             void* stream) {
     using namespace twi;
     if (!frd || !vel || !w) return nofail(TWI_ERR_INVALID, "null array");
-    if (order != 2 && order != 4 && order != 8)
-        return nofail(TWI_ERR_INVALID, "order must be 2, 4 or 8");
+    int s = check_order(order);
+    if (s != TWI_OK) return s;
     const int ne = order / 2, nx = dimx - order, nz = dimy - order;
     if (nx < 1 || nz < 1 || nt < 1)
         return nofail(TWI_ERR_INVALID, "dimx, dimy must exceed order and nt >= 1");
     if (!(h > 0.f) || !(dt > 0.f)) return nofail(TWI_ERR_INVALID, "h and dt must be positive");
-    const int isx = static_cast<int>(sx / h), isy = static_cast<int>(sy / h);
-    const int iry = static_cast<int>(ry / h);
-    if (!(sx >= 0.f) || !(sy >= 0.f) || isx >= nx || isy >= nz)
-        return nofail(TWI_ERR_INVALID, "shot position outside the model");
-    if (!(ry >= 0.f) || iry + ne >= dimy)
-        return nofail(TWI_ERR_INVALID, "receiver row outside the grid");
+    int host_coords[3];   // padded source row, source column, receiver row
+    s = shot_cells(sx, sy, ry, h, nx, nz, ne, dimy, &host_coords[0], &host_coords[1], &host_coords[2]);
+    if (s != TWI_OK) return s;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
 
     // layout inside the fixed scratch: velocity slot, 4 wavefield slots
-    // (slot 0 stays zero), wavelet, shot cells, error word
-    const int pitch = (dimx + kTileX - 1) / kTileX * kTileX;
-    const size_t slot_bytes = (size_t)pitch * dimy * 4;
+    // (slot 0 stays zero), wavelet, shot cells, error word; sizes in 64 bits
+    // so that no grid overflows before it is rejected
+    const long long pitch_ll = ((long long)dimx + kTileX - 1) / kTileX * kTileX;
+    const long long slot_ll = pitch_ll * dimy * 4;
+    if (slot_ll > (long long)kNoAllocScratchBytes)
+        return nofail(TWI_ERR_INVALID,
+                      "grid too large for the no-allocation scratch: one wavefield of " +
+                          std::to_string(dimx) + " x " + std::to_string(dimy) + " cells needs " +
+                          std::to_string(slot_ll) + " bytes, the fixed scratch holds " +
+                          std::to_string(kNoAllocScratchBytes));
+    const int pitch = (int)pitch_ll;
+    const size_t slot_bytes = (size_t)slot_ll;
     const size_t off_vpad = 0;
     const size_t off_fields = up256(off_vpad + slot_bytes);
     const size_t off_wav = up256(off_fields + 4 * slot_bytes);
@@ -136,14 +100,12 @@ extern "C" int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const 
                           " (5 * roundup(dimx,128) * dimy * 4 + nt * 4 bytes plus a few hundred)");
 
     unsigned char* base = nullptr;
-    int s = scratch_address(&base);
+    s = scratch_address(&base);
     if (s != TWI_OK) return s;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     float* vpad = reinterpret_cast<float*>(base + off_vpad);
     float* fields = reinterpret_cast<float*>(base + off_fields);
     int* coords = reinterpret_cast<int*>(base + off_coords);
     int* err = reinterpret_cast<int*>(base + off_err);
-    const int host_coords[3] = {isy + ne, isx + ne, iry + ne};
 
 #define NOALLOC_CUDA(expr)                                                                     \
     do {                                                                                       \
@@ -162,9 +124,9 @@ extern "C" int twi_fdm_forward_only_noalloc(float* frd, const float* vel, const 
     const LaunchShape shape{4, 4};
     const int TZ = 16, HZ = zhalo(order);
     CUtensorMap tm_u2, tm_u1, tm_vel;
-    if ((s = encode(&tm_u2, fields, dimx, dimy, 4, pitch, kBoxX, TZ + 2 * HZ)) != TWI_OK) return s;
-    if ((s = encode(&tm_u1, fields, dimx, dimy, 4, pitch, kTileX, TZ)) != TWI_OK) return s;
-    if ((s = encode(&tm_vel, vpad, dimx, dimy, 0, pitch, kTileX, TZ)) != TWI_OK) return s;
+    if ((s = make_map(&tm_u2, fields, dimx, dimy, 4, pitch, kBoxX, TZ + 2 * HZ)) != TWI_OK) return s;
+    if ((s = make_map(&tm_u1, fields, dimx, dimy, 4, pitch, kTileX, TZ)) != TWI_OK) return s;
+    if ((s = make_map(&tm_vel, vpad, dimx, dimy, 0, pitch, kTileX, TZ)) != TWI_OK) return s;
     NOALLOC_CUDA(prepare_step(order, true, shape));
 
     StepArgs a{};
