@@ -44,10 +44,7 @@ def _load_shot(ftrue: str, index: int, data_type: str, shape=None) -> np.ndarray
         return data
     if data_type == "npy":
         return np.load(path)
-    if data_type == "su":
-        from pkrh.io import su   # the reference's optional SU reader (third-party)
-        return su.fromfile(path, key="data")
-    raise ValueError(f"unknown data_type {data_type!r} (bin | binary | npy | su)")
+    raise ValueError(f"unknown data_type {data_type!r} (bin | binary | npy)")
 
 
 class TimeDataset(torch.utils.data.Dataset):
