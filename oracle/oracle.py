@@ -31,6 +31,15 @@ class OracleError(RuntimeError):
     pass
 
 
+def reference_root() -> str | None:
+    """The TorchWI checkout the reference build reads: $REFROOT, else a
+    directory named ``reference`` beside this repository; None when neither
+    holds the ``torchwi`` package."""
+    cand = os.environ.get("REFROOT") or os.path.join(os.path.dirname(os.path.dirname(_HERE)),
+                                                      "reference")
+    return cand if os.path.isdir(os.path.join(cand, "torchwi")) else None
+
+
 def build(ref: bool = True) -> None:
     """Compile the checkers with ``make`` (the reference part only when its
     sources are present)."""
@@ -38,8 +47,9 @@ def build(ref: bool = True) -> None:
     if os.path.exists("/usr/bin/g++"):
         env["CXX"] = "/usr/bin/g++"  # some toolchains on PATH lack libgomp
     targets = ["oracle"]
-    refroot = env.get("REFROOT", "/root/reference")
-    if ref and os.path.isdir(os.path.join(refroot, "torchwi")):
+    refroot = reference_root()
+    if ref and refroot is not None:
+        env["REFROOT"] = refroot
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", _HERE, *targets], check=True, env=env)
 

@@ -1,8 +1,8 @@
 """Generate the golden fixtures in this directory by running the REFERENCE
 (TorchWI's own ``Time2d(device='cpu')`` operator and its CPU extension built
-from the reference sources).  Needs the reference tree (default
-/root/reference, override with REFROOT) and a C++ compiler; it is NOT run by
-the tests -- the tests only read the fixtures it wrote.
+from the reference sources).  Needs the reference tree ($REFROOT, else a
+checkout named ``reference`` beside this repository) and a C++ compiler; it
+is NOT run by the tests -- the tests only read the fixtures it wrote.
 
     python tests/golden/make_golden.py
 
@@ -30,7 +30,12 @@ import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFROOT = os.environ.get("REFROOT", "/root/reference")
+REFROOT = os.environ.get("REFROOT") or os.path.join(os.path.dirname(REPO), "reference")
+
+
+def _require_reference():
+    if not os.path.isdir(os.path.join(REFROOT, "torchwi")):
+        raise SystemExit(f"reference tree not found at {REFROOT}: set REFROOT to the TorchWI checkout")
 
 
 def _load_reference():
@@ -97,6 +102,7 @@ def main():
     from torchwi_b200 import synthetic
 
     torch.set_num_threads(os.cpu_count() or 1)
+    _require_reference()
     torchwi = _load_reference()
 
     # -- small full-array fixtures ------------------------------------------------

@@ -2,7 +2,7 @@
 
 Run from anywhere where the reference sources are available:
 
-    python tests/golden/make_rsf_golden.py /root/reference
+    python tests/golden/make_rsf_golden.py [<TorchWI checkout>]
 
 It imports torchwi/io/rsf.py by path (nothing else of the reference), writes
 seeded datasets into tests/golden/rsf/ with relative `in=` paths, and records
@@ -86,4 +86,7 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    here = os.path.dirname(os.path.abspath(__file__))
+    default = os.environ.get("REFROOT") or os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(here))),
+                                                        "reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else default)
