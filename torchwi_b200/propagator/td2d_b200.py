@@ -30,6 +30,26 @@ def _cuda_input(t: torch.Tensor, name: str):
         raise RuntimeError(f"{name} must be float32")
 
 
+def _check_sizes(order, dimx, dimy, nt, grid=(), trace=(), history=(), w=None):
+    """The kernels address every array by the sizes passed in, so each must
+    hold at least that many samples: `grid` arrays dimy*dimx, `trace` arrays
+    (frd, resid) nt*nx with nx = dimx - order, `history` arrays (virt)
+    nt*dimy*dimx, and the wavelet nt.  A shorter array is an error here, not
+    an out-of-bounds access on the device.  (The reference's CUDA path passes
+    an (nt, nx_org) residual with the 16-padded nx when nx_org % 16 != 0,
+    propagator_cuda.cu:142 with TimeFunction.py:128,137; that case stops
+    here.)"""
+    nx, dimxy = int(dimx) - int(order), int(dimx) * int(dimy)
+    need = [(t, n, dimxy) for t, n in grid] + [(t, n, int(nt) * nx) for t, n in trace]
+    need += [(t, n, int(nt) * dimxy) for t, n in history]
+    if w is not None:
+        need.append((w, "w", int(nt)))
+    for t, name, n in need:
+        if t.numel() < n:
+            raise RuntimeError(f"{name} holds {t.numel()} samples; order={order}, dimx={dimx}, "
+                               f"dimy={dimy}, nt={nt} need {n}")
+
+
 def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
@@ -50,6 +70,8 @@ def forward(frd, virt, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, sx, sy
     if not w.is_contiguous():
         raise RuntimeError("w must be contiguous")
     w = w.to(torch.float32)
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((frd, "frd"),),
+                 history=((virt, "source_wavefield"),), w=w)
     with torch.cuda.device(frd.device):
         _run(_capi.lib().twi_fdm_forward(_ptr(frd), _ptr(virt), _ptr(u1), _ptr(u2), _ptr(u3),
                                          _ptr(vpad), _ptr(w), int(order), int(dimx), int(dimy),
@@ -61,6 +83,8 @@ def backward(virt, u1, u2, u3, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
     for t, n in ((virt, "source_wavefield"), (u1, "u1"), (u2, "u2"), (u3, "u3"), (vpad, "vel"),
                  (resid, "resid")):
         _cuda_input(t, n)
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((resid, "resid"),),
+                 history=((virt, "source_wavefield"),))
     grad = torch.zeros_like(vpad)
     with torch.cuda.device(vpad.device):
         _run(_capi.lib().twi_fdm_backward(_ptr(grad), _ptr(virt), _ptr(u1), _ptr(u2), _ptr(u3),

@@ -6,7 +6,7 @@ from __future__ import annotations
 import torch
 
 from .. import _capi
-from .td2d_b200 import _cuda_input, _ptr, _run, _stream
+from .td2d_b200 import _check_sizes, _cuda_input, _ptr, _run, _stream
 
 
 def forward(frd, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
@@ -15,6 +15,7 @@ def forward(frd, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
     if not w.is_contiguous():
         raise RuntimeError("w must be contiguous")
     w = w.to(torch.float32)
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((frd, "frd"),), w=w)
     with torch.cuda.device(frd.device):
         _run(_capi.lib().twi_fdm_forward_only(_ptr(frd), _ptr(u1), _ptr(u2), _ptr(u3),
                                               _ptr(vpad), _ptr(w), int(order), int(dimx),

@@ -116,6 +116,23 @@ def config2(nshots: int = 64, nt: int = 4000, seed: int = 1) -> Survey:
                   vel_start=start.astype(np.float32))
 
 
+def layered_case(nx: int, nz: int, nt: int, nshots: int = 1, seed: int = 11, h: float = 10.0,
+                 dt: float = 1.0e-3) -> Survey:
+    """The config-2 model class (three layers 1800/2500/3200 m/s with seeded
+    undulating interfaces, starting model smoothed with sigma 10 cells) on
+    any grid, e.g. the larger serving grids 2000x600 and 4000x1200; Ricker
+    8 Hz, dt = 1 ms (CFL 0.32), surface shots spread evenly."""
+    from scipy.ndimage import gaussian_filter
+
+    true = _layered(nx, nz, np.random.default_rng(seed))
+    shots_ix = ((np.arange(nshots) + 0.5) * nx / nshots).astype(np.int64)
+    sx = shots_ix.astype(np.float64) * h
+    sy = np.full(nshots, 2 * h)
+    return Survey(f"layered_{nx}x{nz}x{nt}", true.astype(np.float32), h, dt,
+                  ricker(8.0, dt, nt).astype(np.float32), sx, sy, sy.copy(), order=4,
+                  vel_start=gaussian_filter(true, 10.0).astype(np.float32))
+
+
 def config3(nshots: int = 256, nt: int = 6000) -> Survey:
     """Batched shots with checkpointing: the config-2 model class with 256
     shots and nt=6000."""
