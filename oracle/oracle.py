@@ -82,11 +82,13 @@ def _load(path: str) -> ctypes.CDLL:
                 _S = ctypes.POINTER(ctypes.c_int16)
                 lib.twio_exa_forward_f32.argtypes = [_F, _F, _S, _F, _F, _i, _i, _i, _i,
                                                      _f, _f, _f, _f, _f]
+                lib.twio_exa_forward_cuda_order_f32.argtypes = lib.twio_exa_forward_f32.argtypes
                 lib.twio_exa_backward_f32.argtypes = [_F, _F, _S, _F, _F, _i, _i, _i, _i,
                                                       _f, _f, _f]
                 for fn in ("twio_forward_f32", "twio_forward_f64",
                            "twio_backward_f32", "twio_backward_f64",
-                           "twio_exa_forward_f32", "twio_exa_backward_f32"):
+                           "twio_exa_forward_f32", "twio_exa_forward_cuda_order_f32",
+                           "twio_exa_backward_f32"):
                     getattr(lib, fn).restype = _i
             else:
                 lib.ref_fdm_forward.argtypes = [_F] * 7 + [_i] * 4 + [_f] * 5
@@ -157,16 +159,19 @@ def twio_backward(virt, vpad, resid, order, dimx, dimy, nt, h, dt, ry,
     return grad
 
 
-def twio_exa_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
-    """Excitation-amplitude forward pass: (frd[nt, nx], exa[dimxy], iexa[dimxy] int16)."""
+def twio_exa_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry, cuda_order=False):
+    """Excitation-amplitude forward pass: (frd[nt, nx], exa[dimxy], iexa[dimxy] int16).
+    cuda_order forms the virtual source with the reference CUDA kernel's
+    operand order (td2d_cuda.cu:189) instead of the CPU propagator's."""
     lib = _load(_ORACLE_SO)
     vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel()
     w = np.ascontiguousarray(w, dtype=np.float32).ravel()
     frd = np.zeros((nt, dimx - order), dtype=np.float32)
     exa = np.zeros(dimx * dimy, dtype=np.float32)
     iexa = np.zeros(dimx * dimy, dtype=np.int16)
-    _check(lib.twio_exa_forward_f32(_ptr(frd), _ptr(exa), iexa.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
-                                    _ptr(vpad), _ptr(w), order, dimx, dimy, nt, h, dt, sx, sy, ry))
+    fn = lib.twio_exa_forward_cuda_order_f32 if cuda_order else lib.twio_exa_forward_f32
+    _check(fn(_ptr(frd), _ptr(exa), iexa.ctypes.data_as(ctypes.POINTER(ctypes.c_int16)),
+              _ptr(vpad), _ptr(w), order, dimx, dimy, nt, h, dt, sx, sy, ry))
     return frd, exa, iexa
 
 

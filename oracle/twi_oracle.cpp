@@ -274,9 +274,14 @@ int backward_impl(T* grad, const T* virt, const T* vel, const T* resid,
 // assigns grad = -exa * lambda at that step.  The reference implements this
 // on CUDA only; the stencil, Keys and virtual-source arithmetic here are
 // those of the CPU propagator, like the rest of this file.
+// cuda_order: form the virtual source as the reference's CUDA kernel writes
+// it, cons/(v*v*v) * ((u^{n+1} - 2u^n) + u^{n-1}) (td2d_cuda.cu:189), instead
+// of the CPU propagator's ((u^{n-1} - 2u^n) + u^{n+1})
+// (propagator_cpu.cpp:70); used only to measure what that order changes.
 template <typename T>
 int exa_forward_impl(T* frd, T* exa, std::int16_t* iexa, const T* vel, const T* w, int order,
-                     int dimx, int dimy, int nt, T h, T dt, T sx, T sy, T ry) {
+                     int dimx, int dimy, int nt, T h, T dt, T sx, T sy, T ry,
+                     bool cuda_order = false) {
     if (order != 2 && order != 4 && order != 8) return 1;
     if (nt > 32767) return 4;
     Grid<T> g(order, dimx, dimy, h, dt);
@@ -299,7 +304,8 @@ int exa_forward_impl(T* frd, T* exa, std::int16_t* iexa, const T* vel, const T* 
 #pragma omp parallel for schedule(static)
         for (std::int64_t i = 0; i < g.dimxy; ++i) {
             const T v3 = vel[i] * vel[i] * vel[i];
-            const T vt = cons / v3 * ((um[i] - T(2) * uo[i]) + up[i]);
+            const T vt = cuda_order ? cons / v3 * ((up[i] - T(2) * uo[i]) + um[i])
+                                    : cons / v3 * ((um[i] - T(2) * uo[i]) + up[i]);
             if (std::fabs(vt) > std::fabs(exa[i])) {
                 exa[i] = vt;
                 iexa[i] = static_cast<std::int16_t>(it);
@@ -348,6 +354,13 @@ int twio_exa_forward_f32(float* frd, float* exa, std::int16_t* iexa, const float
                          const float* w, int order, int dimx, int dimy, int nt, float h, float dt,
                          float sx, float sy, float ry) {
     return exa_forward_impl<float>(frd, exa, iexa, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry);
+}
+
+int twio_exa_forward_cuda_order_f32(float* frd, float* exa, std::int16_t* iexa, const float* vel,
+                                    const float* w, int order, int dimx, int dimy, int nt, float h,
+                                    float dt, float sx, float sy, float ry) {
+    return exa_forward_impl<float>(frd, exa, iexa, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
+                                   true);
 }
 
 int twio_exa_backward_f32(float* grad, const float* exa, const std::int16_t* iexa,

@@ -67,7 +67,7 @@ def _run(torchwi, s, device, shots):
         f = model(par, *xyz)
         (0.5 * torch.sum((f - o) ** 2)).backward()
         obs.append(o.cpu().numpy())
-        frd.append(f.detach().cpu().numpy())
+        frd.append(f.detach().clone().cpu().numpy())   # the reference reuses its frd buffer
     return np.stack(obs), np.stack(frd), par.grad.cpu().numpy()
 
 

@@ -73,6 +73,31 @@ def test_mix_equals_alone(with_obs):
         assert bits_equal(r.result.cpu().numpy(), _alone(models, r).cpu().numpy()), (r.kind, r.model)
 
 
+@pytest.mark.parametrize("with_obs", [False, True])
+def test_request_joining_mid_flight_equals_alone(with_obs):
+    """Requests submitted while others are already on the device join the
+    next ticks (continuous batching) and still give the bits they give
+    alone."""
+    models = _pool()
+    reqs = _requests(models, with_obs)
+    srv = Server(models, h=10.0, dt=1e-3, options=OPTS, max_requests=8)
+    first, late = reqs[:2], reqs[2:]
+    for r in first:
+        srv.submit(r)
+    assert srv.poll(5) == []            # both admitted, 5 of their >= 90 steps done
+    assert srv.engine.pending()[0] == 2
+    for r in late:
+        srv.submit(r)
+        srv.poll(3)                      # admitted beside the ones in flight
+        in_flight, _ = srv.engine.pending()
+        assert in_flight >= 2, "a late request ran alone"
+    while srv.busy():
+        srv.poll(17)
+    for r in reqs:
+        assert r.result is not None
+        assert bits_equal(r.result.cpu().numpy(), _alone(models, r).cpu().numpy()), (r.kind, r.model)
+
+
 def test_memory_limited_admission_and_chunking():
     models = _pool()
     reqs = _requests(models, True)
