@@ -2,9 +2,12 @@
 
 Workload (one "step" = one full gradient of the survey): 64 surface shots on
 the 1000 x 300 three-layer model (h = 10 m, Ricker 8 Hz, dt = 0.8 ms,
-nt = 4000, order 4): forward modelling with checkpoints, L2 residual and
-misfit, checkpointed adjoint with Kahan-summed gradient.  Synthetic data
-(seeded model generator, observed gathers modelled on the true model).
+nt = 4000, order 4): forward modelling that keeps the absorbing-boundary
+cells of every step, L2 residual and misfit, then the backward pass that
+rebuilds the forward field in reverse time and takes the adjoint step in
+the same fused launch, Kahan-summed gradient (--checkpoints: checkpoints
+and a recompute pass instead).  Synthetic data (seeded model generator,
+observed gathers modelled on the true model).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl {b200,reference}]
 
@@ -418,7 +421,8 @@ def run_b200(args):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded 3-layer model, observed gathers modelled on the true model)",
-            "config": {"workload": f"{args.workload}: batched checkpointed FWI gradient, "
+            "config": {"workload": f"{args.workload}: batched FWI gradient "
+                                   f"({'checkpoints' if args.checkpoints else 'boundary saving'}), "
                                    f"{NSHOTS} shots/GPU, 1000x300 cells, nt={NT}, order 4, "
                                    "Keys ABC, Kahan gradient",
                        "global_batch": total_shots, "parallelism": f"shots sharded over {world} GPU(s)",
@@ -608,10 +612,12 @@ def main():
     ap.add_argument("--rz", type=int, default=0)
     ap.add_argument("--time-block", type=int, default=0, help="time steps per launch (0 = plan default)")
     ap.add_argument("--autotune", action="store_true", help="time the launch shapes first and use the fastest")
-    ap.add_argument("--reconstruct", action="store_true",
-                    help="boundary saving + reverse reconstruction instead of checkpoints")
+    ap.add_argument("--checkpoints", action="store_true",
+                    help="checkpoints every --ckpt steps and a recompute pass instead of the default "
+                         "boundary saving with reverse reconstruction")
     ap.add_argument("--split-backward", action="store_true",
-                    help="with --reconstruct: rebuild and adjoint as two launches per step")
+                    help="boundary saving: rebuild and adjoint as two launches per step instead of "
+                         "the fused backward launch")
     ap.add_argument("--plain-shots", type=int, default=4)
     ap.add_argument("--profile-reps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
@@ -625,10 +631,11 @@ def main():
     ap.add_argument("--ticks", type=int, default=64)
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "serve"],
                     help="config2: the 64-shot gradient (default, the contract line); "
-                         "config3: 256 shots, nt=6000, checkpoint every 50 steps; "
+                         "config3: 256 shots, nt=6000 (with --checkpoints: a checkpoint every 50 steps); "
                          "config4: 32 uneven models in HBM-sized waves")
     ap.add_argument("--models", type=int, default=0, help="config4: first N models only")
     args = ap.parse_args()
+    args.reconstruct = not args.checkpoints
     if args.workload == "config3":
         NSHOTS, NT = 256, 6000
         args.ckpt = args.ckpt or 50

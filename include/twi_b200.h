@@ -128,7 +128,7 @@ typedef struct twi_problem {
     int accumulate;       /* 0: Kahan-compensated FP32 over steps and shots;
                              1: plain FP32 per shot, summed in shot order (the
                              reference's order: bit-identical gradients) */
-    int shots_per_cta;    /* shots sharing one velocity tile in a CTA; 0 = choose
+    int shots_per_cta;    /* shots sharing one velocity tile in a CTA, 1..32; 0 = choose
                              (4, and 8 for adjoint launches) */
     int rows_per_warp;    /* 2, 4 or 8 (2: not with time_block 2); 0 = choose
                              (4, and 2 for one-step adjoint launches) */
@@ -155,6 +155,12 @@ typedef struct twi_problem {
                              within its FP32 tolerance, not bit for bit (1 and 2 give
                              the same bits).  One step per launch; plan-level calls
                              only */
+    int persistent;       /* 1: every pass (or checkpoint segment) of twi_forward and
+                             twi_gradient is one persistent launch: CTAs take
+                             (step, shot group, tile) work items in step order and
+                             wait, with bounded waits, for the group's previous
+                             step; 0: one launch per time step.  The same bits
+                             either way; not with time_block 2 */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */

@@ -13,8 +13,9 @@ shot-summed gradient of 0.5*sum((frd-obs)^2), accumulated shot by shot as
 the reference's inversion loop does, plus norms:
   grid_4000x1200 -- one shot, nt=2000 (row pitch 4096 on the GPU);
   grid_2000x600  -- one shot, nt=4500 (more than 4000 steps);
-  survey_256     -- 256 shots on the 1000x300 config-2 model, nt=500
-                    (checkpoint intervals of 50 steps give 10 segments).
+  survey_256     -- 256 shots on a 1000x300 model of the config-2 class,
+                    dt=0.8 ms, nt=500 (checkpoint intervals of 50 steps give
+                    10 segments).
 
 The reference's full propagator cannot run the two single-shot grids: it
 stores the virtual-source history at virt[it*dimxy + i] with 32-bit int
@@ -81,7 +82,8 @@ def main():
     cases = {
         "grid_4000x1200": (lambda: synthetic.layered_case(4000, 1200, 2000, nshots=1, seed=41), "oracle"),
         "grid_2000x600": (lambda: synthetic.layered_case(2000, 600, 4500, nshots=1, seed=42), "oracle"),
-        "survey_256": (lambda: synthetic.config2(nshots=256, nt=500), "reference"),
+        "survey_256": (lambda: synthetic.layered_case(1000, 300, 500, nshots=256, seed=43, dt=0.8e-3),
+                       "reference"),
     }
     out = {}
     for name, (make, source) in cases.items():

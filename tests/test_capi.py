@@ -104,6 +104,29 @@ def test_shots_per_cta_per_mode(spc, nshots, expect):
     L.twi_plan_destroy(h)
 
 
+def test_shots_per_cta_is_bounded():
+    for spc in (-1, 33):
+        st, _ = _create(shots_per_cta=spc, nshots=64)
+        assert st == _capi.TWI_ERR_INVALID
+        assert "shots_per_cta" in _capi.last_error()
+    st, h = _create(shots_per_cta=32, nshots=64)
+    assert st == _capi.TWI_OK
+    _capi.lib().twi_plan_destroy(h)
+
+
+def test_persistent_plans_run_one_step_per_item():
+    st, _ = _create(persistent=1, time_block=2)
+    assert st == _capi.TWI_ERR_INVALID
+    assert "persistent" in _capi.last_error()
+    for kw in (dict(persistent=1), dict(persistent=1, reconstruct=1), dict(persistent=1, forward_only=1)):
+        st, h = _create(**kw)
+        assert st == _capi.TWI_OK, kw
+        lay = _capi.Layout()
+        assert _capi.lib().twi_plan_layout(h, ctypes.byref(lay)) == 0
+        assert lay.time_block == 1
+        _capi.lib().twi_plan_destroy(h)
+
+
 def test_two_rows_per_warp_runs_one_step_per_launch():
     st, h = _create(rows_per_warp=2, time_block=2)
     assert st == _capi.TWI_ERR_INVALID

@@ -4,7 +4,7 @@ configurations, against hashes written from the reference
 
 * a 4000 x 1200 shot with nt = 2000 (row pitch 4096, 32 tile columns);
 * a 2000 x 600 shot with nt = 4500 (more steps than config 2);
-* 256 shots on the config-2 model with a checkpoint every 50 steps.
+* 256 shots on a 1000 x 300 model with a checkpoint every 50 steps.
 
 Bar: gathers and plain-sum gradients bit-identical to the reference (for the
 two single-shot grids the reference's own propagator overflows its 32-bit
@@ -65,7 +65,7 @@ def test_large_grid_shot(golden, case, make):
 
 def test_256_shot_survey_checkpoint_every_50(golden):
     rec = golden["survey_256"]
-    s = synthetic.config2(nshots=256, nt=500)
+    s = synthetic.layered_case(1000, 300, 500, nshots=256, seed=43, dt=0.8e-3)
     dev = torch.device("cuda")
 
     def plan(**kw):

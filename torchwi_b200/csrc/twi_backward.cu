@@ -22,9 +22,11 @@
 // step kernel's (twi_cell.cuh), so the result equals the reverse launch
 // followed by the adjoint launch bit for bit.
 #include <atomic>
+#include <type_traits>
 
 #include "twi_cell.cuh"
 #include "twi_kernels.h"
+#include "twi_persist.cuh"
 #include "twi_ptx.cuh"
 #include "twi_tile.cuh"
 
@@ -137,16 +139,16 @@ __device__ __forceinline__ void update4(const float4 (&win)[ORDER + 1], const fl
     }
 }
 
+// One CTA of one backward step: `cta` indexes the step's CTAs, boundary
+// CTAs first, then the interior tiles.
 template <int ORDER, bool EXACT, int RZ, int WZ>
-__global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
-backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_p,
-                const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ StepArgs a,
-                const int nbc) {
+__device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUtensorMap* tm_p,
+                                              const CUtensorMap* tm_vel, const StepArgs& a,
+                                              const int nbc, const int cta) {
     using S = BackSmem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
 
     const int ngroups = (a.nshots + a.spc - 1) / a.spc;
-    const int cta = blockIdx.x;
     if (cta < nbc * ngroups) {
         backward_boundary<ORDER, EXACT>(a, cta, nbc);
         return;
@@ -171,10 +173,20 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
     const int nloc = min(a.spc, a.nshots - s_begin);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+    // the group's source cells, wavelet samples and receiver rows, read once
+    __shared__ int sh_src_r[kMaxShotsPerCta], sh_src_c[kMaxShotsPerCta], sh_rec_r[kMaxShotsPerCta];
+    __shared__ float sh_wamp[kMaxShotsPerCta];
+    if (threadIdx.x < nloc) {
+        const int s = s_begin + threadIdx.x;
+        sh_src_r[threadIdx.x] = a.src_rc[2 * s];
+        sh_src_c[threadIdx.x] = a.src_rc[2 * s + 1];
+        sh_rec_r[threadIdx.x] = a.rec_row[s];
+        sh_wamp[threadIdx.x] = a.wav[(long long)s * a.wav_stride + a.it];
+    }
     if (threadIdx.x == 0) {
-        prefetch_tmap(&tm_c);
-        prefetch_tmap(&tm_p);
-        prefetch_tmap(&tm_vel);
+        prefetch_tmap(tm_c);
+        prefetch_tmap(tm_p);
+        prefetch_tmap(tm_vel);
 #pragma unroll
         for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
         fence_barrier_init();
@@ -186,14 +198,14 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
         mbar_arrive_expect_tx(b, S::STAGE_TX);
-        tma_load_3d(st, &tm_c, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
-        tma_load_3d(st + S::C_FLOATS, &tm_p, x0, z0, a.prev_base + s * a.prev_stride, b);
-        tma_load_3d(st + S::FIELD_FLOATS, &tm_c, x0 - kHaloX, z0 - HZ, a.lcur_base + s * a.lcur_stride, b);
-        tma_load_3d(st + S::FIELD_FLOATS + S::C_FLOATS, &tm_p, x0, z0, a.lprev_base + s * a.lprev_stride, b);
+        tma_load_3d(st, tm_c, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
+        tma_load_3d(st + S::C_FLOATS, tm_p, x0, z0, a.prev_base + s * a.prev_stride, b);
+        tma_load_3d(st + S::FIELD_FLOATS, tm_c, x0 - kHaloX, z0 - HZ, a.lcur_base + s * a.lcur_stride, b);
+        tma_load_3d(st + S::FIELD_FLOATS + S::C_FLOATS, tm_p, x0, z0, a.lprev_base + s * a.lprev_stride, b);
     };
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
-        tma_load_2d(vs, &tm_vel, x0, z0, &bar[0]);
+        tma_load_2d(vs, tm_vel, x0, z0, &bar[0]);
         for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
     }
 
@@ -202,6 +214,8 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
     const int cs = kHaloX + 4 * lane;    // its column in a haloed row
     const bool col_ok = c < a.dimx;
     const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
+    // every lane of the tile on interior columns (CTA-uniform)
+    const bool tile_interior = x0 >= NE && x0 + kTileX <= a.dimx - NE;
     bool cell_in[4];                     // per-cell interior column mask
 #pragma unroll
     for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
@@ -251,9 +265,8 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
         const float* lc_s = uc_s + S::FIELD_FLOATS;                     // lambda^it, haloed
         const float* lp_s = lc_s + S::C_FLOATS;                         // lambda^{it+1}
 
-        const int src_r = a.src_rc[2 * s], src_c = a.src_rc[2 * s + 1];
-        const float wamp = a.wav[(long long)s * a.wav_stride + a.it];
-        const int rec_r = a.rec_row[s];
+        const int src_r = sh_src_r[k], src_c = sh_src_c[k], rec_r = sh_rec_r[k];
+        const float wamp = sh_wamp[k];
 
         {
             const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
@@ -284,13 +297,11 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
             wu[2 * NE] = ld4(uc_s + (rl + HZ + NE) * kBoxX + cs);
             wl[2 * NE] = ld4(lc_s + (rl + HZ + NE) * kBoxX + cs);
             const long long roff = (long long)r * a.pitch + c;
-            if (r < NE) {
-                // free surface: both fields stay zero (the reference never writes these rows)
-                if (col_ok) {
-                    *reinterpret_cast<float4*>(un_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
-                    *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            } else {
+            // One interior row.  FAST: a row of interior cells only (interior
+            // tile, not a pad row, neither the source nor the receiver row),
+            // so no per-cell or per-row special case is tested.
+            auto interior_row = [&](auto fast_tag) {
+                constexpr bool FAST = decltype(fast_tag)::value;
                 // ---- u^{it-1}: the forward update run backwards
                 const float cu[4] = {wu[NE].x, wu[NE].y, wu[NE].z, wu[NE].w};
                 float Lu[NE], Ru[NE];
@@ -299,7 +310,7 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
                 const float up[4] = {up4.x, up4.y, up4.z, up4.w};
                 // u^{it+1} with the source that step `it` added taken off again
                 float ui[4] = {up[0], up[1], up[2], up[3]};
-                if (r == src_r && src_c >= c && src_c < c + 4) {
+                if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
                     const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
                     for (int m = 0; m < 4; ++m)
@@ -320,7 +331,7 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
                 const float lp[4] = {lp4.x, lp4.y, lp4.z, lp4.w};
                 float lo[4];
                 update4<ORDER, EXACT>(wl, cl, Ll, Rl, lp, vvreg[rr], lo);
-                if (r == rec_r) {   // adjoint source on the receiver row
+                if (!FAST && r == rec_r) {   // adjoint source on the receiver row
                     const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
                     const float* rs = a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
 #pragma unroll
@@ -332,7 +343,7 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
                 }
 
                 // pad columns belong to the boundary CTAs: store interior cells only
-                if (cols_interior) {
+                if (FAST || cols_interior) {
                     *reinterpret_cast<float4*>(un_slot + roff) = make_float4(uo[0], uo[1], uo[2], uo[3]);
                     *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(lo[0], lo[1], lo[2], lo[3]);
                 } else {
@@ -345,7 +356,7 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
                 if (kahan) {
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        if (cell_in[m]) {
+                        if (FAST || cell_in[m]) {
                             const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
                             float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
                             kahan_add(sm, cm, grad_term<EXACT>(vt, lo[m]));
@@ -357,12 +368,23 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
                     float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + roff;
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        if (cell_in[m]) {
+                        if (FAST || cell_in[m]) {
                             const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
                             g[m] = __fadd_rn(g[m], grad_term<EXACT>(vt, lo[m]));
                         }
                     }
                 }
+            };
+            if (r < NE) {
+                // free surface: both fields stay zero (the reference never writes these rows)
+                if (col_ok) {
+                    *reinterpret_cast<float4*>(un_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
+                    *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            } else if (tile_interior && r != src_r && r != rec_r) {
+                interior_row(std::true_type{});
+            } else {
+                interior_row(std::false_type{});
             }
 #pragma unroll
             for (int j = 0; j < 2 * NE; ++j) wu[j] = wu[j + 1], wl[j] = wl[j + 1];
@@ -385,6 +407,27 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
     }
 }
 
+template <int ORDER, bool EXACT, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
+backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_p,
+                const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ StepArgs a,
+                const int nbc) {
+    backward_body<ORDER, EXACT, RZ, WZ>(&tm_c, &tm_p, &tm_vel, a, nbc, blockIdx.x);
+}
+
+// All backward steps of a pass in one launch (twi_persist.cuh).
+template <int ORDER, bool EXACT, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
+backward_kernel_persistent(const __grid_constant__ CUtensorMap tm_c, const __grid_constant__ CUtensorMap tm_p,
+                           const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ PersistLaunch P) {
+    extern __shared__ unsigned char smem_raw[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    persistent_loop(P, bars, 1 + BackSmem<ORDER, RZ, WZ>::STAGES, [&](const StepArgs& a, int cta) {
+        backward_body<ORDER, EXACT, RZ, WZ>(&tm_c, &tm_p, &tm_vel, a, P.nbc, cta);
+    });
+}
+
 template <int ORDER, int RZ, int WZ>
 int back_ctas_of(const StepArgs& a, int* nbc_out) {
     using S = BackSmem<ORDER, RZ, WZ>;
@@ -399,7 +442,7 @@ int back_ctas_of(const StepArgs& a, int* nbc_out) {
 
 template <int ORDER, bool EXACT, int RZ>
 cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtensorMap* tv,
-                     const StepArgs* a, cudaStream_t st) {
+                     const StepArgs* a, const PersistLaunch* pl, cudaStream_t st) {
     using S = BackSmem<ORDER, RZ, 4>;
     static std::atomic<unsigned long long> configured{0};   // one bit per device
     int dev = 0;
@@ -409,7 +452,18 @@ cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtenso
         e = cudaFuncSetAttribute(backward_kernel<ORDER, EXACT, RZ, 4>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(backward_kernel_persistent<ORDER, EXACT, RZ, 4>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+        if (e != cudaSuccess) return e;
         configured.fetch_or(1ull << dev, std::memory_order_relaxed);
+    }
+    if (pl) {
+        int grid = 0;
+        e = persistent_grid(backward_kernel_persistent<ORDER, EXACT, RZ, 4>, 128, S::BYTES,
+                            (long long)pl->nsteps * pl->ngroups * pl->per_group, &grid);
+        if (e != cudaSuccess) return e;
+        backward_kernel_persistent<ORDER, EXACT, RZ, 4><<<dim3((unsigned)grid), 128, S::BYTES, st>>>(*tc, *tp, *tv, *pl);
+        return cudaGetLastError();
     }
     if (!a) return cudaSuccess;   // configure only
     int nbc = 0;
@@ -421,18 +475,19 @@ cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtenso
 
 template <int ORDER, bool EXACT>
 cudaError_t back_shape(int rz, const CUtensorMap* tc, const CUtensorMap* tp, const CUtensorMap* tv,
-                       const StepArgs* a, cudaStream_t st) {
-    if (rz == 2) return back_one<ORDER, EXACT, 2>(tc, tp, tv, a, st);
-    if (rz == 4) return back_one<ORDER, EXACT, 4>(tc, tp, tv, a, st);
+                       const StepArgs* a, const PersistLaunch* pl, cudaStream_t st) {
+    if (rz == 2) return back_one<ORDER, EXACT, 2>(tc, tp, tv, a, pl, st);
+    if (rz == 4) return back_one<ORDER, EXACT, 4>(tc, tp, tv, a, pl, st);
     return cudaErrorInvalidValue;
 }
 
 cudaError_t back_dispatch(int order, bool exact, int rz, const CUtensorMap* tc, const CUtensorMap* tp,
-                          const CUtensorMap* tv, const StepArgs* a, cudaStream_t st) {
+                          const CUtensorMap* tv, const StepArgs* a, const PersistLaunch* pl,
+                          cudaStream_t st) {
     switch (order) {
-        case 2: return exact ? back_shape<2, true>(rz, tc, tp, tv, a, st) : back_shape<2, false>(rz, tc, tp, tv, a, st);
-        case 4: return exact ? back_shape<4, true>(rz, tc, tp, tv, a, st) : back_shape<4, false>(rz, tc, tp, tv, a, st);
-        case 8: return exact ? back_shape<8, true>(rz, tc, tp, tv, a, st) : back_shape<8, false>(rz, tc, tp, tv, a, st);
+        case 2: return exact ? back_shape<2, true>(rz, tc, tp, tv, a, pl, st) : back_shape<2, false>(rz, tc, tp, tv, a, pl, st);
+        case 4: return exact ? back_shape<4, true>(rz, tc, tp, tv, a, pl, st) : back_shape<4, false>(rz, tc, tp, tv, a, pl, st);
+        case 8: return exact ? back_shape<8, true>(rz, tc, tp, tv, a, pl, st) : back_shape<8, false>(rz, tc, tp, tv, a, pl, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -453,12 +508,19 @@ cudaError_t launch_backward(int order, bool exact, LaunchShape shape, const CUte
                             const CUtensorMap& tm_p, const CUtensorMap& tm_vel, const StepArgs& a,
                             cudaStream_t stream) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
-    return back_dispatch(order, exact, shape.rows_per_warp, &tm_c, &tm_p, &tm_vel, &a, stream);
+    return back_dispatch(order, exact, shape.rows_per_warp, &tm_c, &tm_p, &tm_vel, &a, nullptr, stream);
+}
+
+cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape, const CUtensorMap& tm_c,
+                                       const CUtensorMap& tm_p, const CUtensorMap& tm_vel,
+                                       const PersistLaunch& P, cudaStream_t stream) {
+    if (shape.warps != 4) return cudaErrorInvalidValue;
+    return back_dispatch(order, exact, shape.rows_per_warp, &tm_c, &tm_p, &tm_vel, nullptr, &P, stream);
 }
 
 cudaError_t prepare_backward(int order, bool exact, LaunchShape shape) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
-    return back_dispatch(order, exact, shape.rows_per_warp, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return back_dispatch(order, exact, shape.rows_per_warp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
 }  // namespace twi

@@ -91,6 +91,18 @@ struct StepArgs {
     int lnext_base, lnext_stride;
 };
 
+// A persistent launch (twi_persist.cuh): `nsteps` consecutive time steps of
+// one plan pass in one launch, steps[s] holding the arguments of step s
+// (device memory).  Each step has `ngroups` shot groups of `per_group` CTAs
+// (`nbc` boundary CTAs, then the interior tiles).  ticket and count[ngroups]
+// must be zero when the launch starts.
+struct PersistLaunch {
+    const StepArgs* steps;
+    int nsteps, ngroups, per_group, nbc;
+    unsigned* ticket;
+    unsigned* count;
+};
+
 // The part of a time step's arguments that changes from step to step.
 struct StepDyn {
     int it;
@@ -164,6 +176,9 @@ __host__ __device__ constexpr int zhalo(int order) { return order / 2; }
 // and this many cells per thread, ahead of the interior tiles in the grid.
 constexpr int kBoundaryCellsPerThread = 4;
 constexpr int kThreads = 128;
+// Largest shot group of one CTA (its shots' source and receiver cells are
+// staged in shared memory by the fused backward kernel).
+constexpr int kMaxShotsPerCta = 32;
 
 // Two-step launches (twi_step2.cu): output tiles of kTile2X columns.  tm_un
 // is a tensor map over the field slots with a (136, 4*rows_per_warp + 2*order)
@@ -189,6 +204,17 @@ cudaError_t launch_backward(int order, bool exact, LaunchShape shape, const CUte
                             const CUtensorMap& tm_p, const CUtensorMap& tm_vel, const StepArgs& a,
                             cudaStream_t stream);
 cudaError_t prepare_backward(int order, bool exact, LaunchShape shape);
+
+// Persistent launches (twi_persist.cuh): every step of P in one launch; the
+// CTAs of one step are those a one-step launch of P.steps[0] would use
+// (step_ctas / backward_ctas give nbc and the total).
+cudaError_t launch_step_persistent(int order, bool exact, StepMode mode, LaunchShape shape,
+                                   const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
+                                   const CUtensorMap& tm_vel, const PersistLaunch& P,
+                                   cudaStream_t stream);
+cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape, const CUtensorMap& tm_c,
+                                       const CUtensorMap& tm_p, const CUtensorMap& tm_vel,
+                                       const PersistLaunch& P, cudaStream_t stream);
 
 // Store n host integers into device memory through kernel parameters
 // (chunks of 2048), ordered on `stream` without a host synchronisation.

@@ -1,0 +1,140 @@
+// twi_persist.cuh -- the work loop of persistent launches: one launch runs
+// many time steps of one plan pass.
+//
+// Work items are (step, shot group, CTA of that group) in step-major order
+// and are handed out by an atomic ticket, so a CTA only ever holds an item
+// once it is running.  Before an item of step s runs, the CTA waits until
+// every item of step s-1 of the same shot group has signalled completion on
+// that group's counter (counters grow monotonically within a launch: step s
+// may start once the counter reaches s * items_per_group).  Because an item
+// waits only for items with smaller tickets, the earliest unfinished item
+// always has everything it needs: the launch cannot deadlock, whatever the
+// grid size and however many CTAs are resident.  Within a group the three
+// rotating wavefield slots are safe: step s overwrites the slot of step
+// s-3's output, which only steps s-2 and s-1 of the same group read, and
+// those have finished.
+//
+// Every wait is bounded: after kWaitLimitNs without progress, or as soon as
+// another CTA has raised the error word, the CTA raises bit 1 of the word
+// and leaves; the launch then ends quickly and the host sees the error.
+//
+// Memory ordering: a finished item's stores are released (every thread
+// fences, then one thread adds to the counter); the waiting thread acquires
+// the counter and then fences between the generic and the async (TMA) proxy,
+// so the tensor loads of the next item see the data; the CTA barrier that
+// follows orders the other threads' plain loads after the acquire.
+#pragma once
+
+#include <cstdint>
+
+#include "twi_kernels.h"
+#include "twi_ptx.cuh"
+
+namespace twi {
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ int ld_volatile_s32(const int* p) {
+    return *reinterpret_cast<const volatile int*>(p);
+}
+
+__device__ __forceinline__ void fence_proxy_async_global() {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Thread 0 only: wait until *count >= target.  False when the wait ran out
+// (bit 1 of *err raised) or another CTA reported an error.
+__device__ __forceinline__ bool wait_count(const unsigned* count, unsigned target, int* err) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 0;; ++i) {
+        if (ld_acquire_u32(count) >= target) return true;
+        if (ld_volatile_s32(err) != 0) return false;
+        if ((i & 63u) == 63u && globaltimer_ns() - t0 > kWaitLimitNs) {
+            atomicOr(err, 2);
+            return false;
+        }
+        __nanosleep(64);
+    }
+}
+
+// The persistent work loop.  `body(args, cta)` runs one CTA of a step as a
+// non-persistent launch would (cta indexes the step's CTAs, boundary CTAs
+// first); `nbars` mbarriers at `bars` are initialised by the body of an
+// interior item and invalidated here after it.
+template <typename Body>
+__device__ __forceinline__ void persistent_loop(const PersistLaunch& P, uint64_t* bars, int nbars,
+                                                Body body) {
+    __shared__ unsigned s_ticket;
+    __shared__ int s_go, s_more;   // uniform decisions, written by thread 0
+    __shared__ StepArgs s_args;
+    const unsigned per_step = (unsigned)P.ngroups * (unsigned)P.per_group;
+    const unsigned total = per_step * (unsigned)P.nsteps;
+    if (threadIdx.x == 0) s_ticket = atomicAdd(P.ticket, 1u);
+    __syncthreads();
+    unsigned item = s_ticket;
+    while (item < total) {
+        const unsigned step = item / per_step;
+        const unsigned rem = item - step * per_step;
+        const int grp = (int)(rem / (unsigned)P.per_group);
+        const int j = (int)(rem - (unsigned)grp * (unsigned)P.per_group);
+        const StepArgs* src = P.steps + step;
+        if (threadIdx.x == 0) {
+            s_ticket = atomicAdd(P.ticket, 1u);   // the next item, claimed early
+            bool ok = ld_volatile_s32(src->err) == 0;
+            if (ok && step > 0) ok = wait_count(P.count + grp, step * (unsigned)P.per_group, src->err);
+            fence_proxy_async_global();
+            s_go = ok ? 1 : 0;
+        }
+        // this step's arguments (the body's first barrier orders the copy)
+        {
+            const int* s = reinterpret_cast<const int*>(src);
+            int* d = reinterpret_cast<int*>(&s_args);
+            for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / 4); i += blockDim.x) d[i] = s[i];
+        }
+        __syncthreads();
+        const unsigned next = s_ticket;
+        if (!s_go) return;
+        // boundary CTAs first, then the interior tiles, as in a one-step launch
+        const int cta = j < P.nbc ? grp * P.nbc + j : P.nbc * P.ngroups + grp * (P.per_group - P.nbc) + (j - P.nbc);
+        body(s_args, cta);
+        fence_proxy_async_global();   // this item's stores, before any later tensor load
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (j >= P.nbc)
+                for (int b = 0; b < nbars; ++b) mbar_inval(&bars[b]);
+            s_more = ld_volatile_s32(s_args.err) == 0;
+            if (s_more) atomicAdd(P.count + grp, 1u);
+        }
+        __syncthreads();
+        if (!s_more) return;
+        item = next;
+    }
+}
+
+// Host: the grid of a persistent launch -- as many CTAs as can be resident
+// at once on the current device (occupancy x SMs), at most one per work item.
+template <typename Kernel>
+cudaError_t persistent_grid(Kernel kernel, int threads, size_t smem_bytes, long long items, int* grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem_bytes);
+    if (e != cudaSuccess) return e;
+    if (items < 1) return cudaErrorInvalidConfiguration;
+    long long g = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    if (g > items) g = items;
+    *grid = (int)g;
+    return cudaSuccess;
+}
+
+}  // namespace twi

@@ -186,6 +186,13 @@ struct twi_plan {
     size_t off_vel = 0, off_wav = 0, off_frd = 0, off_grad = 0, off_coords = 0, off_err = 0,
            off_vpad = 0, off_fields = 0, off_virt = 0, off_acc = 0, off_comp = 0, off_exa = 0,
            off_iexa = 0, off_mpart = 0, off_bnd = 0, total = 0;
+    // persistent launches: one launch per run of same-mode steps, reading the
+    // steps' arguments from tables in the workspace (uploaded outside any
+    // graph capture by sync_table) and two counters regions
+    bool persist = false;
+    enum { kTabForward = 0, kTabForwardSave = 1, kTabForwardResid = 2, kTabGradient = 3, kTables = 4 };
+    size_t off_tab[kTables] = {}, tab_cap[kTables] = {}, off_cnt = 0;
+    std::vector<StepArgs> tab_host[kTables];
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
@@ -445,6 +452,71 @@ struct twi_plan {
 
     // `obs` / `misfit` (both or neither): the gathers region receives the
     // residual modelled - observed and *misfit = 0.5 * sum(residual^2).
+    static int forward_table(bool save, const float* obs) {
+        return obs ? kTabForwardResid : save ? kTabForwardSave : kTabForward;
+    }
+
+    // Bring step table k in line with `steps` (a copy from host memory on
+    // `st`, only when the content changed).  Runs outside graph capture.
+    int sync_table(int k, const std::vector<Step>& steps, cudaStream_t st) {
+        std::vector<StepArgs> v;
+        v.reserve(steps.size());
+        for (const Step& t : steps) v.push_back(t.a);
+        if (v.size() > tab_cap[k]) return fail(TWI_ERR_STATE, "step table too small");
+        if (v.size() == tab_host[k].size() &&
+            std::memcmp(v.data(), tab_host[k].data(), v.size() * sizeof(StepArgs)) == 0)
+            return TWI_OK;
+        TWI_CUDA(cudaMemcpyAsync(ws + off_tab[k], v.data(), v.size() * sizeof(StepArgs),
+                                 cudaMemcpyHostToDevice, st));
+        tab_host[k] = std::move(v);
+        return TWI_OK;
+    }
+
+    // One persistent launch of `n` steps of one mode whose arguments are the
+    // device table entries dev[0..n).
+    int launch_persistent(StepMode mode, const StepArgs& a0, const StepArgs* dev, int n,
+                          cudaStream_t st) const {
+        const bool adj = (mode == kModeAdjoint || mode == kModeBackward) && rz_adj != rz;
+        const LaunchShape sh = default_shape(adj ? rz_adj : rz);
+        int nbc = 0;
+        const int total = mode == kModeBackward ? backward_ctas(p.order, sh.rows_per_warp, a0, &nbc)
+                                                : step_ctas(p.order, sh, a0, &nbc);
+        const int ngroups = (a0.nshots + a0.spc - 1) / a0.spc;
+        if (total <= 0 || ngroups < 1 || total % ngroups != 0)
+            return fail(TWI_ERR_INVALID, "persistent launch too large");
+        unsigned* cnt = reinterpret_cast<unsigned*>(ws + off_cnt);
+        const PersistLaunch L{dev, n, ngroups, total / ngroups, nbc, cnt, cnt + 1};
+        TWI_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(1 + ngroups) * sizeof(unsigned), st));
+        const CUtensorMap& t2 = adj ? ta_u2 : tm_u2;
+        const CUtensorMap& t1 = adj ? ta_u1 : tm_u1;
+        const CUtensorMap& tv = adj ? ta_vel : tm_vel;
+        cudaError_t e = mode == kModeBackward
+                            ? launch_backward_persistent(p.order, p.exact != 0, sh, t2, t1, tv, L, st)
+                            : launch_step_persistent(p.order, p.exact != 0, mode, sh, t2, t1, tv, L, st);
+        if (e != cudaSuccess)
+            return fail(TWI_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(e));
+        return TWI_OK;
+    }
+
+    // The steps of table k, one persistent launch per run of the same mode.
+    int launch_table(int k, const std::vector<Step>& steps, cudaStream_t st) const {
+        const StepArgs* dev = reinterpret_cast<const StepArgs*>(ws + off_tab[k]);
+        for (size_t i = 0; i < steps.size();) {
+            size_t j = i + 1;
+            while (j < steps.size() && steps[j].mode == steps[i].mode) ++j;
+            TWI_TRY(launch_persistent(steps[i].mode, steps[i].a, dev + i, (int)(j - i), st));
+            i = j;
+        }
+        return TWI_OK;
+    }
+
+    // The forward / gradient step lists exactly as the enqueue functions
+    // build them (for the step tables).
+    void forward_list(bool save, const float* obs, std::vector<Step>& steps) const {
+        forward_steps(save, steps, tb == 2);
+        for (Step& t : steps) t.a.obs = obs;
+    }
+
     int enqueue_forward(bool save, cudaStream_t st, const float* obs = nullptr,
                         double* misfit = nullptr) const {
         if (save && exa) {   // the maxima start from zero
@@ -452,10 +524,11 @@ struct twi_plan {
             TWI_CUDA(cudaMemsetAsync(ws + off_iexa, 0, (size_t)p.nshots * slot_elems * 2, st));
         }
         std::vector<Step> steps;
-        forward_steps(save, steps, tb == 2);
-        for (Step& s : steps) {
-            s.a.obs = obs;
-            TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
+        forward_list(save, obs, steps);
+        if (persist) {
+            TWI_TRY(launch_table(forward_table(save, obs), steps, st));
+        } else {
+            for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
         }
         if (misfit) {
             cudaError_t e = launch_misfit(F(off_frd), (long long)p.nshots * p.nt * p.nx,
@@ -469,7 +542,11 @@ struct twi_plan {
         TWI_TRY(gradient_prologue(st));
         std::vector<Step> steps;
         gradient_steps(steps, tb == 2);
-        for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
+        if (persist) {
+            TWI_TRY(launch_table(kTabGradient, steps, st));
+        } else {
+            for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
+        }
         return gradient_epilogue(st);
     }
 
@@ -524,6 +601,8 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
         return fail(TWI_ERR_INVALID, "two time steps per launch need rows_per_warp 4 or 8");
     if (p.ckpt_interval < 0 || p.ckpt_interval == 1)
         return fail(TWI_ERR_INVALID, "ckpt_interval must be 0 (choose) or >= 2");
+    if (p.shots_per_cta < 0 || p.shots_per_cta > kMaxShotsPerCta)
+        return fail(TWI_ERR_INVALID, "shots_per_cta must be 0 (choose) or 1.." + std::to_string(kMaxShotsPerCta));
 
     twi_plan* P = new twi_plan();
     P->p = p;
@@ -570,6 +649,12 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     }
     if (P->fused_back && P->rz_adj == 8) P->rz_adj = 4;   // the fused kernel has 2- and 4-row tiles
     P->tb = P->exa || P->recon ? 1 : p.time_block == 0 ? kDefaultTimeBlock : p.time_block;
+    if (p.persistent < 0 || p.persistent > 1 || (p.persistent == 1 && P->tb == 2)) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "persistent must be 0 or 1, and persistent launches run one step per work item "
+                                     "(time_block 2 is not available with them)");
+    }
+    P->persist = p.persistent == 1;
     P->rot = P->tb == 2 ? 4 : 3;
     if (P->recon) {   // no checkpoints: one segment, one virtual-source slot per shot
         P->K = p.nt;
@@ -601,6 +686,16 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
     P->off_iexa = take(P->exa ? (size_t)p.nshots * P->slot_elems * 2 : 0);
     P->off_mpart = take(P->gradient ? (size_t)kMisfitBlocks * sizeof(double) : 0);
     P->off_bnd = take(P->recon ? (size_t)(p.nt + 1) * p.nshots * P->nb * 4 : 0);
+    if (P->persist) {
+        for (int k = 0; k < twi_plan::kTables; ++k) {
+            const bool grad_table = k == twi_plan::kTabGradient || k == twi_plan::kTabForwardSave ||
+                                    k == twi_plan::kTabForwardResid;
+            P->tab_cap[k] = grad_table && !P->gradient ? 0
+                          : k == twi_plan::kTabGradient ? (size_t)2 * p.nt : (size_t)p.nt;
+            P->off_tab[k] = take(P->tab_cap[k] * sizeof(StepArgs));
+        }
+        P->off_cnt = take((size_t)(1 + p.nshots) * sizeof(unsigned));
+    }
     P->total = off;
     *out = P;
     return TWI_OK;
@@ -713,6 +808,11 @@ int twi_forward(twi_plan* P, int save_checkpoints, void* stream) {
     if (save && !P->gradient)
         return fail(TWI_ERR_STATE, "a forward-only plan keeps no checkpoints");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (P->persist) {
+        std::vector<twi_plan::Step> steps;
+        P->forward_list(save, nullptr, steps);
+        TWI_TRY(P->sync_table(twi_plan::forward_table(save, nullptr), steps, st));
+    }
     TWI_TRY(P->run(&P->g_fwd[save ? 1 : 0], st,
                    [&](cudaStream_t s) { return P->enqueue_forward(save, s); }));
     P->have_ckpt = save;
@@ -732,6 +832,11 @@ int twi_forward_residual(twi_plan* P, const float* observed, double* misfit, voi
     P->res_obs = observed;
     P->res_misfit = misfit;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (P->persist) {
+        std::vector<twi_plan::Step> steps;
+        P->forward_list(true, observed, steps);
+        TWI_TRY(P->sync_table(twi_plan::kTabForwardResid, steps, st));
+    }
     TWI_TRY(P->run(&P->g_fwd_res, st,
                    [&](cudaStream_t s) { return P->enqueue_forward(true, s, observed, misfit); }));
     P->have_ckpt = true;
@@ -743,6 +848,11 @@ int twi_gradient(twi_plan* P, void* stream) {
     if (!P->have_ckpt)
         return fail(TWI_ERR_STATE, "twi_gradient needs a preceding twi_forward(save_checkpoints=1)");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (P->persist) {
+        std::vector<twi_plan::Step> steps;
+        P->gradient_steps(steps, P->tb == 2);
+        TWI_TRY(P->sync_table(twi_plan::kTabGradient, steps, st));
+    }
     return P->run(&P->g_bwd, st, [&](cudaStream_t s) { return P->enqueue_gradient(s); });
 }
 
@@ -854,7 +964,8 @@ std::vector<twi_problem> tune_candidates(const twi_problem& p) {
         for (int rz : {0, 2, 4, 8}) {
             if (p.rows_per_warp && rz != p.rows_per_warp) continue;
             for (int tb : {1, 2}) {
-                if ((p.time_block && tb != p.time_block) || ((p.exa || p.reconstruct || rz == 2) && tb == 2))
+                if ((p.time_block && tb != p.time_block) ||
+                    ((p.exa || p.reconstruct || p.persistent || rz == 2) && tb == 2))
                     continue;
                 twi_problem q = p;
                 q.nt = 8;

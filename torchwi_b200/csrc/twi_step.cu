@@ -23,6 +23,7 @@
 
 #include "twi_cell.cuh"
 #include "twi_kernels.h"
+#include "twi_persist.cuh"
 #include "twi_ptx.cuh"
 #include "twi_tile.cuh"
 
@@ -635,6 +636,20 @@ step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
     }
 }
 
+// Persistent launches: many time steps of one plan pass in one launch
+// (twi_persist.cuh), each work item running one CTA of one step.
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
+step_kernel_persistent(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
+                       const __grid_constant__ CUtensorMap tm_vel, const __grid_constant__ PersistLaunch P) {
+    extern __shared__ unsigned char smem_raw[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    persistent_loop(P, bars, 1 + Smem<ORDER, RZ, WZ>::STAGES, [&](const StepArgs& a, int cta) {
+        step_body<ORDER, EXACT, MODE, RZ, WZ>(&tm_u2, &tm_u1, &tm_vel, a, dyn_of(a), P.nbc, cta);
+    });
+}
+
 // Engine launches: the CTA ranges and the per-step integers come from the
 // kernel parameters, the static arguments of each request and kernel mode
 // from a template resident in device memory.
@@ -678,6 +693,7 @@ struct LaunchReq {
     long long nctas = 0;
     const CUtensorMap* tmaps = nullptr;
     const EngineLaunch* engine = nullptr;
+    const PersistLaunch* persist = nullptr;
     bool multi = false;
     bool configure_only = false;
 };
@@ -709,6 +725,9 @@ cudaError_t configure_one() {
     e = cudaFuncSetAttribute(step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
     if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+    if (e != cudaSuccess) return e;
     if constexpr (MODE <= kModeAdjoint) {   // multi-plan kernels: modes 0-2
         e = cudaFuncSetAttribute(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
@@ -725,6 +744,15 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     using S = Smem<ORDER, RZ, WZ>;
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
     if (e != cudaSuccess || q.configure_only) return e;
+    if (q.persist) {
+        const long long items = (long long)q.persist->nsteps * q.persist->ngroups * q.persist->per_group;
+        int grid = 0;
+        e = persistent_grid(step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>, WZ * 32, S::BYTES, items, &grid);
+        if (e != cudaSuccess) return e;
+        step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>
+            <<<dim3((unsigned)grid), WZ * 32, S::BYTES, stream>>>(*q.t2, *q.t1, *q.tv, *q.persist);
+        return cudaGetLastError();
+    }
     if (q.engine || q.multi) {
         if constexpr (MODE > kModeAdjoint) {
             return cudaErrorInvalidValue;   // excitation amplitude, reverse: single-plan launches only
@@ -922,6 +950,15 @@ cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape 
                               const CUtensorMap* tmaps, cudaStream_t stream) {
     LaunchReq q;
     q.multi = true, q.jobs = jobs, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    return launch_req(order, exact, mode, shape, q, stream);
+}
+
+cudaError_t launch_step_persistent(int order, bool exact, StepMode mode, LaunchShape shape,
+                                   const CUtensorMap& tm_u2, const CUtensorMap& tm_u1,
+                                   const CUtensorMap& tm_vel, const PersistLaunch& P,
+                                   cudaStream_t stream) {
+    LaunchReq q;
+    q.t2 = &tm_u2, q.t1 = &tm_u1, q.tv = &tm_vel, q.persist = &P;
     return launch_req(order, exact, mode, shape, q, stream);
 }
 

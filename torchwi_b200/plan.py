@@ -50,6 +50,9 @@ class PlanOptions:
     split_backward: with reconstruct, run the rebuild and the adjoint step
                  as two launches per step with the virtual source passed
                  through memory (the same bits; kept for comparison).
+    persistent:  run each pass (each checkpoint segment's recompute and
+                 adjoint phase) as ONE persistent launch instead of one
+                 launch per time step (the same bits).
     """
 
     exact: bool = True
@@ -63,6 +66,7 @@ class PlanOptions:
     time_block: int = 0
     reconstruct: bool = False
     split_backward: bool = False
+    persistent: bool = False
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -93,7 +97,8 @@ def autotune(nx, nz, nshots, order=4, h=10.0, dt=1e-3, options: PlanOptions | No
     o = options or PlanOptions()
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     key = (dev.index, nx, nz, nshots, order, o.exact, o.accumulate, o.forward_only, o.exa,
-           o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct, o.split_backward)
+           o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct, o.split_backward,
+           o.persistent)
     if key in _TUNED:
         return _TUNED[key]
     import dataclasses
@@ -139,7 +144,8 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    use_graphs=int(bool(o.use_graphs)), wavelet_per_shot=int(bool(wavelet_per_shot)),
                    forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)),
                    time_block=int(o.time_block),
-                   reconstruct=(2 if o.split_backward else 1) if o.reconstruct else 0)
+                   reconstruct=(2 if o.split_backward else 1) if o.reconstruct else 0,
+                   persistent=int(bool(o.persistent)))
 
 
 class ShotPlan:

@@ -78,7 +78,7 @@ def config1(nshots: int = 10) -> Survey:
                   meta={"anomaly_sign": float(sign), "ext": ext})
 
 
-def _layered(nx: int, nz: int, rng: np.random.Generator) -> np.ndarray:
+def _layered(nx: int, nz: int, rng: np.random.Generator, depths=None) -> np.ndarray:
     x = np.arange(nx, dtype=np.float64)
 
     def undulation():
@@ -90,8 +90,9 @@ def _layered(nx: int, nz: int, rng: np.random.Generator) -> np.ndarray:
             u += amp * np.sin(2 * np.pi * x / lam + ph)
         return np.clip(u, -5.0, 5.0)
 
-    z1 = nz / 3.0 + undulation()
-    z2 = 2.0 * nz / 3.0 + undulation()
+    d1, d2 = depths if depths is not None else (nz / 3.0, 2.0 * nz / 3.0)
+    z1 = d1 + undulation()
+    z2 = d2 + undulation()
     iz = np.arange(nz, dtype=np.float64)[None, :]
     v = np.where(iz < z1[:, None], 1800.0, np.where(iz < z2[:, None], 2500.0, 3200.0))
     return v
@@ -118,13 +119,22 @@ def config2(nshots: int = 64, nt: int = 4000, seed: int = 1) -> Survey:
 
 def layered_case(nx: int, nz: int, nt: int, nshots: int = 1, seed: int = 11, h: float = 10.0,
                  dt: float = 1.0e-3) -> Survey:
-    """The config-2 model class (three layers 1800/2500/3200 m/s with seeded
-    undulating interfaces, starting model smoothed with sigma 10 cells) on
-    any grid, e.g. the larger serving grids 2000x600 and 4000x1200; Ricker
-    8 Hz, dt = 1 ms (CFL 0.32), surface shots spread evenly."""
+    """Parity workload on any grid (e.g. 2000x600, 4000x1200): the config-2
+    model class -- three layers 1800/2500/3200 m/s with seeded undulating
+    interfaces, here at 100 and 200 cells depth whatever nz is, so that
+    reflections return within a few thousand steps -- plus a +-5 %
+    near-surface perturbation along the whole line (period 150 cells, centred
+    20 cells down), so that even the direct and diving waves of every shot
+    differ between the true model and the starting model (the true model
+    smoothed with sigma 10 cells).  Ricker 8 Hz, surface shots spread
+    evenly."""
     from scipy.ndimage import gaussian_filter
 
-    true = _layered(nx, nz, np.random.default_rng(seed))
+    true = _layered(nx, nz, np.random.default_rng(seed), depths=(min(100.0, nz / 3.0),
+                                                                  min(200.0, 2.0 * nz / 3.0)))
+    ix = np.arange(nx, dtype=np.float64)[:, None]
+    iz = np.arange(nz, dtype=np.float64)[None, :]
+    true = true * (1.0 + 0.05 * np.sin(2 * np.pi * ix / 150.0) * np.exp(-(iz - 20.0) ** 2 / (2 * 8.0 ** 2)))
     shots_ix = ((np.arange(nshots) + 0.5) * nx / nshots).astype(np.int64)
     sx = shots_ix.astype(np.float64) * h
     sy = np.full(nshots, 2 * h)
