@@ -47,12 +47,19 @@ MODE_NAMES = {0: "forward step", 1: "recompute step (+virtual source)", 2: "adjo
 TRAFFIC_SHOTS = 64                      # shots per launch of the captures in profiles/traffic.json
 
 
-def _launches_per_gradient(nt, K, time_block, backward="checkpoints"):
+def _launches_per_gradient(nt, K, time_block, backward="checkpoints", persistent=False):
     """Kernel launches of one gradient: model padding, the forward steps, the
     two misfit passes, the backward steps (per checkpoint segment its
     recompute and adjoint steps; with boundary saving one fused launch per
     step, or a rebuild and an adjoint launch), the gradient reduction.
-    Two-step launches cover pairs of steps; an odd remainder runs alone."""
+    Two-step launches cover pairs of steps; an odd remainder runs alone.
+    Persistent launches cover each run of steps of one kernel mode: the
+    forward pass, each segment's recompute and adjoint phases, the fused
+    backward pass."""
+    if persistent:
+        segs = (nt + K - 1) // K
+        back = 1 if backward == "fused" else 2 * nt if backward == "split" else 2 * segs
+        return 1 + 1 + 2 + back + 1
     per = (lambda n: (n + 1) // 2) if time_block == 2 else (lambda n: n)
     if backward == "fused":
         back = nt
@@ -234,7 +241,7 @@ def run_b200(args):
     opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
                        shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True,
                        time_block=args.time_block, reconstruct=args.reconstruct,
-                       split_backward=args.split_backward)
+                       split_backward=args.split_backward, persistent=args.persistent)
     fused = args.reconstruct and not args.split_backward
     tuned_ms = None
     if args.autotune:   # outside the timed region
@@ -415,7 +422,7 @@ def run_b200(args):
     if rank == 0:
         launches = args.steps * _launches_per_gradient(
             NT, plan.layout.ckpt_interval, plan.layout.time_block,
-            "fused" if fused else "split" if args.reconstruct else "checkpoints")
+            "fused" if fused else "split" if args.reconstruct else "checkpoints", args.persistent)
         line = {
             "metric": "shot-gradients/s", "value": value, "unit": "shot-gradients/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -433,6 +440,8 @@ def run_b200(args):
                        "adjoint_rows_per_warp": plan.layout.adjoint_rows_per_warp,
                        "adjoint_shots_per_cta": plan.layout.adjoint_shots_per_cta,
                        "time_block": plan.layout.time_block,
+                       "launches": "one persistent launch per pass" if args.persistent
+                                   else "one launch per time step (CUDA graph)",
                        "autotuned": bool(args.autotune),
                        "adjoint_wavefield": ("boundary saving, reverse reconstruction, "
                                              + ("rebuild and adjoint launches" if args.split_backward
@@ -615,6 +624,8 @@ def main():
     ap.add_argument("--checkpoints", action="store_true",
                     help="checkpoints every --ckpt steps and a recompute pass instead of the default "
                          "boundary saving with reverse reconstruction")
+    ap.add_argument("--persistent", action="store_true",
+                    help="one persistent launch per pass instead of one launch per time step")
     ap.add_argument("--split-backward", action="store_true",
                     help="boundary saving: rebuild and adjoint as two launches per step instead of "
                          "the fused backward launch")

@@ -730,6 +730,7 @@ int twi_plan_bind(twi_plan* P, void* workspace, size_t bytes) {
         return fail(TWI_ERR_INVALID, "workspace must be 256-byte aligned");
     P->drop_graphs();
     P->ws = static_cast<char*>(workspace);
+    for (auto& t : P->tab_host) t.clear();   // the new workspace holds no step tables yet
     TWI_CUDA(cudaGetDevice(&P->device));
     TWI_CUDA(prepare_step(P->p.order, P->p.exact != 0, default_shape(P->rz)));
     const int HZ = zhalo(P->p.order);

@@ -20,6 +20,7 @@
 // general per-cell path.  The top NE rows are the free surface: always 0.
 #include <atomic>
 #include <cstdio>
+#include <type_traits>
 
 #include "twi_cell.cuh"
 #include "twi_kernels.h"
@@ -162,6 +163,16 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     const int nloc = min(a.spc, a.nshots - s_begin);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
+    // the group's source cells, wavelet samples and receiver rows, read once
+    __shared__ int sh_src_r[kMaxShotsPerCta], sh_src_c[kMaxShotsPerCta], sh_rec_r[kMaxShotsPerCta];
+    __shared__ float sh_wamp[kMaxShotsPerCta];
+    if (threadIdx.x < nloc) {
+        const int s = s_begin + threadIdx.x;
+        sh_src_r[threadIdx.x] = MODE != kModeAdjoint ? a.src_rc[2 * s] : -1;
+        sh_src_c[threadIdx.x] = MODE != kModeAdjoint ? a.src_rc[2 * s + 1] : -1;
+        sh_wamp[threadIdx.x] = MODE != kModeAdjoint ? a.wav[(long long)s * a.wav_stride + d.it] : 0.f;
+        sh_rec_r[threadIdx.x] = a.rec_row[s];
+    }
     if (threadIdx.x == 0) {
         prefetch_tmap(tm_u2p);
         prefetch_tmap(tm_u1p);
@@ -192,6 +203,8 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     const bool col_ok = c < a.dimx;
     // the lane's four columns are all interior (stencil) columns
     const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
+    // every lane of the tile on interior columns (CTA-uniform)
+    const bool tile_interior = x0 >= NE && x0 + kTileX <= a.dimx - NE;
     bool cell_in[4];                     // per-cell interior column mask
 #pragma unroll
     for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
@@ -262,14 +275,8 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         const float* u2s = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         const float* u1s = u2s + S::U2_FLOATS;
 
-        int src_r = -1, src_c = -1;
-        float wamp = 0.f;
-        if constexpr (MODE != kModeAdjoint) {
-            src_r = a.src_rc[2 * s];
-            src_c = a.src_rc[2 * s + 1];
-            wamp = a.wav[(long long)s * a.wav_stride + d.it];
-        }
-        const int rec_r = a.rec_row[s];
+        const int src_r = sh_src_r[k], src_c = sh_src_c[k], rec_r = sh_rec_r[k];
+        const float wamp = sh_wamp[k];
 
         // virtual source of this step for the warp's rows (adjoint); only the
         // virtual-source accumulations read it -- the excitation-amplitude
@@ -390,178 +397,185 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     }
                 }
             } else {
-                float out[4];
-                // backwards, u^{it+1} stands where u^{n-1} did, with the source
-                // that step `it` added taken off again
-                float ui[4] = {um[0], um[1], um[2], um[3]};
-                if constexpr (MODE == kModeReverse) {
-                    if (r == src_r && src_c >= c && src_c < c + 4) {
-                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-#pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (c + m == src_c) ui[m] = __fsub_rn(um[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
-                    }
-                }
-#pragma unroll
-                for (int m = 0; m < 4; ++m) {
-                    float lf[NE], rt[NE], up[NE], dn[NE];
-#pragma unroll
-                    for (int dist = 1; dist <= NE; ++dist) {
-                        const int jl = m - dist, jr = m + dist;
-                        lf[dist - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
-                        rt[dist - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
-                        up[dist - 1] = comp(win[NE - dist], m);
-                        dn[dist - 1] = comp(win[NE + dist], m);
-                    }
-                    out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
-                                                           comp(vvreg[rr], m));
+                // One interior row.  FAST: interior tile, neither the source
+                // nor the receiver row, so no per-cell or per-row special case
+                // is tested.
+                auto interior_row = [&](auto fast_tag) {
+                    constexpr bool FAST = decltype(fast_tag)::value;
+                    float out[4];
+                    // backwards, u^{it+1} stands where u^{n-1} did, with the source
+                    // that step `it` added taken off again
+                    float ui[4] = {um[0], um[1], um[2], um[3]};
                     if constexpr (MODE == kModeReverse) {
-                        if (d.it < 2) out[m] = 0.f;   // u^0 = u^{-1} = 0 exactly
-                    }
-                }
-                // sources land on interior cells only (validated on the host)
-                if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
-                    if (r == src_r && src_c >= c && src_c < c + 4) {
-                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                        if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
+                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (c + m == src_c)
-                                out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
-                    }
-                } else if constexpr (MODE == kModeAdjoint) {
-                    if (r == rec_r) {
-                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-                        const float* rs =
-                            a.resid + (long long)s * a.resid_stride + (long long)d.it * a.nx;
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) {
-                            const int cc = c + m;
-                            if (cc >= NE && cc < NE + a.nx)
-                                out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
+                            for (int m = 0; m < 4; ++m)
+                                if (c + m == src_c) ui[m] = __fsub_rn(um[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
                         }
                     }
-                }
-
-                // pad columns belong to the boundary CTAs: store interior cells only
-                if (cols_interior) {
-                    *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
-                } else {
 #pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        if (cell_in[m]) dst[m] = out[m];
-                }
-
-                if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
-                    if (a.frd != nullptr && r == rec_r) {
-                        const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
-                        float* g = a.frd + o;
-                        if (a.obs != nullptr) {   // the residual, one rounding like frd - obs
-                            const float* ob = a.obs + o;
+                    for (int m = 0; m < 4; ++m) {
+                        float lf[NE], rt[NE], up[NE], dn[NE];
+#pragma unroll
+                        for (int dist = 1; dist <= NE; ++dist) {
+                            const int jl = m - dist, jr = m + dist;
+                            lf[dist - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
+                            rt[dist - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
+                            up[dist - 1] = comp(win[NE - dist], m);
+                            dn[dist - 1] = comp(win[NE + dist], m);
+                        }
+                        out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
+                                                               comp(vvreg[rr], m));
+                        if constexpr (MODE == kModeReverse) {
+                            if (d.it < 2) out[m] = 0.f;   // u^0 = u^{-1} = 0 exactly
+                        }
+                    }
+                    // sources land on interior cells only (validated on the host)
+                    if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
+                        if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
+                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+#pragma unroll
+                            for (int m = 0; m < 4; ++m)
+                                if (c + m == src_c)
+                                    out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
+                        }
+                    } else if constexpr (MODE == kModeAdjoint) {
+                        if (!FAST && r == rec_r) {
+                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                            const float* rs =
+                                a.resid + (long long)s * a.resid_stride + (long long)d.it * a.nx;
 #pragma unroll
                             for (int m = 0; m < 4; ++m) {
                                 const int cc = c + m;
-                                if (cc >= NE && cc < NE + a.nx) g[cc - NE] = __fsub_rn(out[m], ob[cc - NE]);
-                            }
-                        } else {
-#pragma unroll
-                            for (int m = 0; m < 4; ++m) {
-                                const int cc = c + m;
-                                if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                                if (cc >= NE && cc < NE + a.nx)
+                                    out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
                             }
                         }
                     }
-                }
 
-                if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
-                    float vo[4];
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        vo[m] = MODE == kModeReverse
-                                    ? virt_from_coef<EXACT>(comp(qreg[rr], m), out[m], c4[m], um[m])
-                                    : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
-                    float* p = a.virt_out +
-                               (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
-                               (long long)r * a.virt_pitch + c;
-                    if (cols_interior && a.virt_vec4) {
-                        *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
+                    // pad columns belong to the boundary CTAs: store interior cells only
+                    if (FAST || cols_interior) {
+                        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
                     } else {
 #pragma unroll
                         for (int m = 0; m < 4; ++m)
-                            if (cell_in[m]) p[m] = vo[m];
+                            if (cell_in[m]) dst[m] = out[m];
                     }
-                }
 
-                if constexpr (MODE == kModeExaForward) {
-                    const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
-                    float4 ev = ld4(a.exa + e0);
-                    short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
-                    bool changed = false;
+                    if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
+                        if (!FAST && a.frd != nullptr && r == rec_r) {
+                            const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
+                            float* g = a.frd + o;
+                            if (a.obs != nullptr) {   // the residual, one rounding like frd - obs
+                                const float* ob = a.obs + o;
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        if (!cell_in[m]) continue;
-                        const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
-                        if (fabsf(vt) > fabsf(comp(ev, m))) {
-                            set_comp(ev, m, vt);
-                            if (m == 0) iv.x = static_cast<short>(d.it);
-                            else if (m == 1) iv.y = static_cast<short>(d.it);
-                            else if (m == 2) iv.z = static_cast<short>(d.it);
-                            else iv.w = static_cast<short>(d.it);
-                            changed = true;
-                        }
-                    }
-                    if (changed) {
-                        if (cols_interior) {
-                            *reinterpret_cast<float4*>(a.exa + e0) = ev;
-                            *reinterpret_cast<short4*>(a.iexa + e0) = iv;
-                        } else {   // pad columns belong to the boundary CTAs
-                            const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+                                for (int m = 0; m < 4; ++m) {
+                                    const int cc = c + m;
+                                    if (cc >= NE && cc < NE + a.nx) g[cc - NE] = __fsub_rn(out[m], ob[cc - NE]);
+                                }
+                            } else {
 #pragma unroll
-                            for (int m = 0; m < 4; ++m)
-                                if (cell_in[m]) a.exa[e0 + m] = comp(ev, m), a.iexa[e0 + m] = is[m];
-                        }
-                    }
-                }
-
-                if constexpr (MODE == kModeAdjoint) {
-                    if (a.acc_mode == kAccExa) {
-                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
-                        const short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
-                        const short is[4] = {iv.x, iv.y, iv.z, iv.w};
-                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                                   (long long)r * a.pitch + c;
-#pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (cell_in[m] && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
-                    } else if (a.acc_mode == kAccKahanPerGroup) {
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) {
-                            if (cell_in[m]) {
-                                float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
-                                kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
-                                set_comp(gsum[rr], m, sm);
-                                set_comp(gcmp[rr], m, cm);
+                                for (int m = 0; m < 4; ++m) {
+                                    const int cc = c + m;
+                                    if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                                }
                             }
                         }
-                    } else if (a.acc_mode == kAccPlainPerShot) {
-                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                                   (long long)r * a.pitch + c;
-                        if (cols_interior) {
-                            float4 gv = ld4(g);
+                    }
+
+                    if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
+                        float vo[4];
 #pragma unroll
-                            for (int m = 0; m < 4; ++m)
-                                set_comp(gv, m, __fadd_rn(comp(gv, m),
-                                                          grad_term<EXACT>(comp(vin[rr], m), out[m])));
-                            *reinterpret_cast<float4*>(g) = gv;
+                        for (int m = 0; m < 4; ++m)
+                            vo[m] = MODE == kModeReverse
+                                        ? virt_from_coef<EXACT>(comp(qreg[rr], m), out[m], c4[m], um[m])
+                                        : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                        float* p = a.virt_out +
+                                   (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                   (long long)r * a.virt_pitch + c;
+                        if ((FAST || cols_interior) && a.virt_vec4) {
+                            *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
                         } else {
 #pragma unroll
                             for (int m = 0; m < 4; ++m)
-                                if (cell_in[m])
-                                    g[m] = __fadd_rn(g[m], grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                if (cell_in[m]) p[m] = vo[m];
                         }
                     }
-                }
-            }
 
+                    if constexpr (MODE == kModeExaForward) {
+                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                        float4 ev = ld4(a.exa + e0);
+                        short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                        bool changed = false;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            if (!FAST && !cell_in[m]) continue;
+                            const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                            if (fabsf(vt) > fabsf(comp(ev, m))) {
+                                set_comp(ev, m, vt);
+                                if (m == 0) iv.x = static_cast<short>(d.it);
+                                else if (m == 1) iv.y = static_cast<short>(d.it);
+                                else if (m == 2) iv.z = static_cast<short>(d.it);
+                                else iv.w = static_cast<short>(d.it);
+                                changed = true;
+                            }
+                        }
+                        if (changed) {
+                            if (FAST || cols_interior) {
+                                *reinterpret_cast<float4*>(a.exa + e0) = ev;
+                                *reinterpret_cast<short4*>(a.iexa + e0) = iv;
+                            } else {   // pad columns belong to the boundary CTAs
+                                const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+#pragma unroll
+                                for (int m = 0; m < 4; ++m)
+                                    if (cell_in[m]) a.exa[e0 + m] = comp(ev, m), a.iexa[e0 + m] = is[m];
+                            }
+                        }
+                    }
+
+                    if constexpr (MODE == kModeAdjoint) {
+                        if (a.acc_mode == kAccExa) {
+                            const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                            const short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                            const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+                            float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                       (long long)r * a.pitch + c;
+#pragma unroll
+                            for (int m = 0; m < 4; ++m)
+                                if ((FAST || cell_in[m]) && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
+                        } else if (a.acc_mode == kAccKahanPerGroup) {
+#pragma unroll
+                            for (int m = 0; m < 4; ++m) {
+                                if (FAST || cell_in[m]) {
+                                    float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                                    kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                    set_comp(gsum[rr], m, sm);
+                                    set_comp(gcmp[rr], m, cm);
+                                }
+                            }
+                        } else if (a.acc_mode == kAccPlainPerShot) {
+                            float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                       (long long)r * a.pitch + c;
+                            if (FAST || cols_interior) {
+                                float4 gv = ld4(g);
+#pragma unroll
+                                for (int m = 0; m < 4; ++m)
+                                    set_comp(gv, m, __fadd_rn(comp(gv, m),
+                                                              grad_term<EXACT>(comp(vin[rr], m), out[m])));
+                                *reinterpret_cast<float4*>(g) = gv;
+                            } else {
+#pragma unroll
+                                for (int m = 0; m < 4; ++m)
+                                    if (cell_in[m])
+                                        g[m] = __fadd_rn(g[m], grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                            }
+                        }
+                    }
+                };
+                if (tile_interior && r != src_r && r != rec_r) interior_row(std::true_type{});
+                else interior_row(std::false_type{});
+            }
 #pragma unroll
             for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
         }
