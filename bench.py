@@ -491,7 +491,7 @@ def run_config4(args):
     models = synthetic.config4()
     if args.models:
         models = models[:args.models]
-    opts = PlanOptions(exact=not args.fast, accumulate="kahan")
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan", reconstruct=not args.checkpoints)
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(free * 0.80)
     fps = [footprint_bytes(m.nx, m.nz, m.nt, m.nshots, 4, options=opts) for m in models]
@@ -551,6 +551,7 @@ def run_config4(args):
         del batch, plans, obs, starts
         torch.cuda.empty_cache()
     print(json.dumps({"workload": "config4 uneven batch", "metric": "shot-gradients/s",
+                      "adjoint_wavefield": "checkpoints" if args.checkpoints else "boundary saving, fused backward",
                       "value": shots / (total_ms / 1e3), "unit": "shot-gradients/s",
                       "gcell_per_s": cells / (total_ms / 1e3) / 1e9, "models": len(models),
                       "shots": shots, "ms_total": total_ms, "waves": per_wave,
@@ -565,7 +566,8 @@ def run_serve(args):
     per-request form (each request alone, FIFO) gives the comparison.
     Observed gathers are zero (the residual is the modelled data): the work is
     identical to real data.  The sample size is bounded by --requests,
-    --max-shots and --nt-max so one rate point takes about a minute."""
+    --max-shots and --nt-max (defaults: 12 requests per rate, the config-5
+    ranges of 1-128 shots and nt 2000-8000)."""
     import torch
 
     from torchwi_b200 import PlanOptions, synthetic
@@ -573,7 +575,7 @@ def run_serve(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    opts = PlanOptions(exact=not args.fast, accumulate="kahan")
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan", reconstruct=not args.checkpoints)
     out = []
     for rate in args.rates:
         models_np, reqs_np = synthetic.config5(rate, nreq=args.requests, max_shots=args.max_shots,
@@ -602,6 +604,7 @@ def run_serve(args):
         del srv
         torch.cuda.empty_cache()
     print(json.dumps({"workload": "config5 serving stream", "requests_per_rate": args.requests,
+                      "adjoint_wavefield": "checkpoints" if args.checkpoints else "boundary saving, fused backward",
                       "max_shots": args.max_shots, "nt_range": [args.nt_min, args.nt_max],
                       "grids": [list(g) for g in synthetic.SERVE_GRIDS],
                       "arith": "fast-fp32" if args.fast else "reference-exact",
@@ -635,10 +638,10 @@ def main():
     ap.add_argument("--shots", type=int, default=NSHOTS, help="shots per GPU")
     ap.add_argument("--nt", type=int, default=NT, help="time steps")
     ap.add_argument("--rates", type=float, nargs="+", default=[5.0, 200.0])
-    ap.add_argument("--requests", type=int, default=16)
-    ap.add_argument("--max-shots", type=int, default=32)
+    ap.add_argument("--requests", type=int, default=12)
+    ap.add_argument("--max-shots", type=int, default=128)
     ap.add_argument("--nt-min", type=int, default=2000)
-    ap.add_argument("--nt-max", type=int, default=4000)
+    ap.add_argument("--nt-max", type=int, default=8000)
     ap.add_argument("--ticks", type=int, default=64)
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "serve"],
                     help="config2: the 64-shot gradient (default, the contract line); "

@@ -23,12 +23,16 @@ def _plan(s, opts):
     return p
 
 
-@pytest.mark.parametrize("accumulate,graphs,rz", [("plain", True, 0), ("plain", False, 0),
-                                                  ("kahan", True, 0), ("kahan", False, 0),
-                                                  ("kahan", True, 2)])
-def test_batch_equals_plans_alone(accumulate, graphs, rz):
+@pytest.mark.parametrize("accumulate,graphs,rz,recon", [("plain", True, 0, False), ("plain", False, 0, False),
+                                                        ("kahan", True, 0, False), ("kahan", False, 0, False),
+                                                        ("kahan", True, 2, False), ("plain", True, 0, True),
+                                                        ("kahan", True, 0, True), ("kahan", False, 4, True)])
+def test_batch_equals_plans_alone(accumulate, graphs, rz, recon):
+    """recon: boundary-saving plans, whose backward steps are fused launches
+    (one multi-plan launch of the fused backward kernel per step)."""
     surveys = [synthetic.small_case(order=4, **c) for c in CASES]
-    opts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs, rows_per_warp=rz)
+    opts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs, rows_per_warp=rz,
+                       reconstruct=recon)
     alone = []
     for s in surveys:
         p = _plan(s, opts)

@@ -88,9 +88,12 @@ def test_fused_backward_equals_split_launches(order, accumulate, shape):
     assert np.abs(grads[0]).max() > 0
 
 
-def test_reconstruction_plans_stay_out_of_batches():
+def test_split_backward_plans_stay_out_of_batches():
+    # fused boundary-saving plans batch (tests/test_gpu_batch.py); the form with
+    # separate rebuild and adjoint launches runs through its own plan only
     s = synthetic.small_case(nx=40, nz=20, nt=50, nshots=2)
-    p = _plan(s, reconstruct=True)
+    p = _plan(s, reconstruct=True, split_backward=True)
     p.set_model(torch.from_numpy(s.vel).cuda())
     with pytest.raises(TwiInvalid):
         PlanBatch([p])
+    PlanBatch([_plan(s, reconstruct=True)])

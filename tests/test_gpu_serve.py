@@ -39,9 +39,9 @@ def _requests(models, with_obs):
     return out
 
 
-def _alone(models, r):
+def _alone(models, r, opts=OPTS):
     nx, nz = models[r.model].shape
-    o = PlanOptions(**{**OPTS.__dict__, "forward_only": r.kind == "forward"})
+    o = PlanOptions(**{**opts.__dict__, "forward_only": r.kind == "forward"})
     p = ShotPlan(nx, nz, 10.0, 1e-3, r.nt, 4, nshots=r.nshots, options=o)
     p.set_wavelet(torch.from_numpy(r.w))
     p.set_shots(r.sx, r.sy, r.ry)
@@ -96,6 +96,26 @@ def test_request_joining_mid_flight_equals_alone(with_obs):
     for r in reqs:
         assert r.result is not None
         assert bits_equal(r.result.cpu().numpy(), _alone(models, r).cpu().numpy()), (r.kind, r.model)
+
+
+def test_boundary_saving_requests_mix_equals_alone():
+    """Gradient requests of boundary-saving plans (fused backward steps: one
+    engine launch of the fused kernel per tick for all of them) next to
+    forward requests, some joining mid-flight, give the bits they give
+    alone."""
+    opts = PlanOptions(accumulate="plain", reconstruct=True)
+    models = _pool()
+    reqs = _requests(models, True)
+    srv = Server(models, h=10.0, dt=1e-3, options=opts, max_requests=8)
+    for r in reqs[:3]:
+        srv.submit(r)
+    srv.poll(7)
+    for r in reqs[3:]:
+        srv.submit(r)
+    while srv.busy():
+        srv.poll(13)
+    for r in reqs:
+        assert bits_equal(r.result.cpu().numpy(), _alone(models, r, opts).cpu().numpy()), (r.kind, r.model)
 
 
 def test_memory_limited_admission_and_chunking():

@@ -415,6 +415,37 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
     backward_body<ORDER, EXACT, RZ, WZ>(&tm_c, &tm_p, &tm_vel, a, nbc, blockIdx.x);
 }
 
+// Backward steps of several plans in one launch: CTA ranges of the jobs are
+// contiguous and ascending; a job reads its plan's adjoint-height tensor maps
+// (tmaps[6p + 3 .. 6p + 5]).  The arguments are copied to shared memory so
+// that the body does not re-read them from global memory after its stores.
+template <int ORDER, bool EXACT, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
+backward_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
+                      const CUtensorMap* __restrict__ tmaps) {
+    const int lo = job_of([&](int i) { return jobs[i].cta_begin; }, njobs, (int)blockIdx.x);
+    const MultiJob& J = jobs[lo];
+    const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan + 3;
+    __shared__ StepArgs a;
+    copy_args(a, J.a);
+    backward_body<ORDER, EXACT, RZ, WZ>(tm, tm + 1, tm + 2, a, J.nbc, blockIdx.x - J.cta_begin);
+}
+
+// Engine launches: job ranges and per-step slots from the kernel parameters,
+// the static arguments from the request's resident template.
+template <int ORDER, bool EXACT, int RZ, int WZ>
+__global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
+backward_kernel_engine(const __grid_constant__ EngineLaunch L, const CUtensorMap* __restrict__ tmaps) {
+    const int lo = job_of([&](int i) { return L.cta_begin[i]; }, L.njobs, (int)blockIdx.x);
+    const MultiJob& J = *L.tmpl[lo];
+    const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan + 3;
+    __shared__ StepArgs a;
+    copy_args(a, J.a);
+    if (threadIdx.x == 0) apply_dyn(a, L.dyn[lo]);
+    __syncthreads();
+    backward_body<ORDER, EXACT, RZ, WZ>(tm, tm + 1, tm + 2, a, J.nbc, blockIdx.x - L.cta_begin[lo]);
+}
+
 // All backward steps of a pass in one launch (twi_persist.cuh).
 template <int ORDER, bool EXACT, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
@@ -440,10 +471,27 @@ int back_ctas_of(const StepArgs& a, int* nbc_out) {
     return n > 0x7fffffffLL ? -1 : (int)n;
 }
 
+// One launch request: a single step (tensor maps + args), a persistent pass,
+// a job table or an engine launch; none of them = set the attributes only.
+struct BackReq {
+    const CUtensorMap* tc = nullptr;
+    const CUtensorMap* tp = nullptr;
+    const CUtensorMap* tv = nullptr;
+    const StepArgs* a = nullptr;
+    const PersistLaunch* pl = nullptr;
+    const MultiJob* jobs = nullptr;
+    int njobs = 0;
+    long long nctas = 0;
+    const CUtensorMap* tmaps = nullptr;
+    const EngineLaunch* engine = nullptr;
+};
+
 template <int ORDER, bool EXACT, int RZ>
-cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtensorMap* tv,
-                     const StepArgs* a, const PersistLaunch* pl, cudaStream_t st) {
+cudaError_t back_one(const BackReq& q, cudaStream_t st) {
     using S = BackSmem<ORDER, RZ, 4>;
+    const CUtensorMap *tc = q.tc, *tp = q.tp, *tv = q.tv;
+    const StepArgs* a = q.a;
+    const PersistLaunch* pl = q.pl;
     static std::atomic<unsigned long long> configured{0};   // one bit per device
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -455,7 +503,23 @@ cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtenso
         e = cudaFuncSetAttribute(backward_kernel_persistent<ORDER, EXACT, RZ, 4>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(backward_kernel_multi<ORDER, EXACT, RZ, 4>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(backward_kernel_engine<ORDER, EXACT, RZ, 4>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(S::BYTES));
+        if (e != cudaSuccess) return e;
         configured.fetch_or(1ull << dev, std::memory_order_relaxed);
+    }
+    if (q.jobs || q.engine) {
+        if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+        if (q.engine)
+            backward_kernel_engine<ORDER, EXACT, RZ, 4>
+                <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(*q.engine, q.tmaps);
+        else
+            backward_kernel_multi<ORDER, EXACT, RZ, 4>
+                <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(q.jobs, q.njobs, q.tmaps);
+        return cudaGetLastError();
     }
     if (pl) {
         int grid = 0;
@@ -474,20 +538,17 @@ cudaError_t back_one(const CUtensorMap* tc, const CUtensorMap* tp, const CUtenso
 }
 
 template <int ORDER, bool EXACT>
-cudaError_t back_shape(int rz, const CUtensorMap* tc, const CUtensorMap* tp, const CUtensorMap* tv,
-                       const StepArgs* a, const PersistLaunch* pl, cudaStream_t st) {
-    if (rz == 2) return back_one<ORDER, EXACT, 2>(tc, tp, tv, a, pl, st);
-    if (rz == 4) return back_one<ORDER, EXACT, 4>(tc, tp, tv, a, pl, st);
+cudaError_t back_shape(int rz, const BackReq& q, cudaStream_t st) {
+    if (rz == 2) return back_one<ORDER, EXACT, 2>(q, st);
+    if (rz == 4) return back_one<ORDER, EXACT, 4>(q, st);
     return cudaErrorInvalidValue;
 }
 
-cudaError_t back_dispatch(int order, bool exact, int rz, const CUtensorMap* tc, const CUtensorMap* tp,
-                          const CUtensorMap* tv, const StepArgs* a, const PersistLaunch* pl,
-                          cudaStream_t st) {
+cudaError_t back_dispatch(int order, bool exact, int rz, const BackReq& q, cudaStream_t st) {
     switch (order) {
-        case 2: return exact ? back_shape<2, true>(rz, tc, tp, tv, a, pl, st) : back_shape<2, false>(rz, tc, tp, tv, a, pl, st);
-        case 4: return exact ? back_shape<4, true>(rz, tc, tp, tv, a, pl, st) : back_shape<4, false>(rz, tc, tp, tv, a, pl, st);
-        case 8: return exact ? back_shape<8, true>(rz, tc, tp, tv, a, pl, st) : back_shape<8, false>(rz, tc, tp, tv, a, pl, st);
+        case 2: return exact ? back_shape<2, true>(rz, q, st) : back_shape<2, false>(rz, q, st);
+        case 4: return exact ? back_shape<4, true>(rz, q, st) : back_shape<4, false>(rz, q, st);
+        case 8: return exact ? back_shape<8, true>(rz, q, st) : back_shape<8, false>(rz, q, st);
     }
     return cudaErrorInvalidValue;
 }
@@ -508,19 +569,40 @@ cudaError_t launch_backward(int order, bool exact, LaunchShape shape, const CUte
                             const CUtensorMap& tm_p, const CUtensorMap& tm_vel, const StepArgs& a,
                             cudaStream_t stream) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
-    return back_dispatch(order, exact, shape.rows_per_warp, &tm_c, &tm_p, &tm_vel, &a, nullptr, stream);
+    BackReq q;
+    q.tc = &tm_c, q.tp = &tm_p, q.tv = &tm_vel, q.a = &a;
+    return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
 }
 
 cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape, const CUtensorMap& tm_c,
                                        const CUtensorMap& tm_p, const CUtensorMap& tm_vel,
                                        const PersistLaunch& P, cudaStream_t stream) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
-    return back_dispatch(order, exact, shape.rows_per_warp, &tm_c, &tm_p, &tm_vel, nullptr, &P, stream);
+    BackReq q;
+    q.tc = &tm_c, q.tp = &tm_p, q.tv = &tm_vel, q.pl = &P;
+    return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
+}
+
+cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
+                                  int njobs, long long nctas, const CUtensorMap* tmaps,
+                                  cudaStream_t stream) {
+    if (shape.warps != 4) return cudaErrorInvalidValue;
+    BackReq q;
+    q.jobs = jobs, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
+}
+
+cudaError_t launch_backward_engine(int order, bool exact, LaunchShape shape, const EngineLaunch& L,
+                                   long long nctas, const CUtensorMap* tmaps, cudaStream_t stream) {
+    if (shape.warps != 4) return cudaErrorInvalidValue;
+    BackReq q;
+    q.engine = &L, q.nctas = nctas, q.tmaps = tmaps;
+    return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
 }
 
 cudaError_t prepare_backward(int order, bool exact, LaunchShape shape) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
-    return back_dispatch(order, exact, shape.rows_per_warp, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+    return back_dispatch(order, exact, shape.rows_per_warp, BackReq{}, nullptr);
 }
 
 }  // namespace twi

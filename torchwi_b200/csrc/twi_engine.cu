@@ -61,13 +61,15 @@ struct twi_engine {
     int order = 4;
     bool exact = true;
     LaunchShape shape{4, 4};
+    LaunchShape shape_back{2, 4};   // fused backward steps of boundary-saving requests
+    static constexpr int kModes = 6;   // templates indexed by StepMode
     int max_requests = 0;
     char* ws = nullptr;
     size_t off_tmaps = 0, off_tmpl = 0, total = 0;
     // pinned staging per request slot: its tensor maps and per-mode templates
     struct SlotStage {
-        CUtensorMap tm[3];
-        MultiJob tmpl[3];
+        CUtensorMap tm[kMapsPerPlan];
+        MultiJob tmpl[kModes];
     };
     SlotStage* staging = nullptr;
     std::vector<cudaEvent_t> slot_events;   // per slot: its last upload
@@ -79,7 +81,7 @@ struct twi_engine {
         long long tag = 0;
         int slot = -1;                  // tensor-map / template slot
         std::vector<TwiStep> steps;     // forward steps, then gradient steps
-        int nbc[3] = {0, 0, 0}, ncta[3] = {0, 0, 0};   // per kernel mode
+        int nbc[kModes] = {}, ncta[kModes] = {};   // per kernel mode
         size_t fwd_steps = 0, pos = 0;
         bool started = false;
     };
@@ -89,7 +91,7 @@ struct twi_engine {
     std::deque<long long> completed;    // finished, not yet reported
 
     const MultiJob* tmpl_dev(int slot, int mode) const {
-        return reinterpret_cast<const MultiJob*>(ws + off_tmpl) + 3 * slot + mode;
+        return reinterpret_cast<const MultiJob*>(ws + off_tmpl) + kModes * slot + mode;
     }
 
     int admit(cudaStream_t st) {
@@ -102,7 +104,7 @@ struct twi_engine {
             ENG_CUDA(cudaEventSynchronize(slot_events[R.slot]));
             SlotStage& S = staging[R.slot];
             plan_tensor_maps(R.plan, S.tm);
-            bool seen[3] = {false, false, false};
+            bool seen[kModes] = {};
             for (const TwiStep& t : R.steps) {   // static arguments per kernel mode
                 const int m = static_cast<int>(t.mode);
                 if (seen[m]) continue;
@@ -110,14 +112,16 @@ struct twi_engine {
                 S.tmpl[m] = MultiJob{};
                 S.tmpl[m].a = t.a;
                 S.tmpl[m].plan = R.slot;
-                R.ncta[m] = step_ctas(order, shape, t.a, &R.nbc[m]);
+                R.ncta[m] = t.mode == kModeBackward
+                                ? backward_ctas(order, shape_back.rows_per_warp, t.a, &R.nbc[m])
+                                : step_ctas(order, shape, t.a, &R.nbc[m]);
                 S.tmpl[m].nbc = R.nbc[m];
                 S.tmpl[m].ncta = R.ncta[m];
                 if (R.ncta[m] <= 0) return efail(TWI_ERR_INVALID, "request launch too large");
             }
             // enqueued on the engine's stream: ordered after every kernel that
             // read this slot for an earlier request
-            ENG_CUDA(cudaMemcpyAsync(ws + off_tmaps + 3 * R.slot * sizeof(CUtensorMap), S.tm,
+            ENG_CUDA(cudaMemcpyAsync(ws + off_tmaps + kMapsPerPlan * R.slot * sizeof(CUtensorMap), S.tm,
                                      sizeof(S.tm), cudaMemcpyHostToDevice, st));
             ENG_CUDA(cudaMemcpyAsync(const_cast<MultiJob*>(tmpl_dev(R.slot, 0)), S.tmpl,
                                      sizeof(S.tmpl), cudaMemcpyHostToDevice, st));
@@ -146,7 +150,8 @@ struct twi_engine {
 
     int launch(EngineLaunch& L, StepMode m, long long nctas, cudaStream_t st) {
         const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
-        ENG_CUDA(launch_step_engine(order, exact, m, shape, L, nctas, tm, st));
+        ENG_CUDA(m == kModeBackward ? launch_backward_engine(order, exact, shape_back, L, nctas, tm, st)
+                                    : launch_step_engine(order, exact, m, shape, L, nctas, tm, st));
         L.njobs = 0;
         return TWI_OK;
     }
@@ -157,7 +162,7 @@ struct twi_engine {
             if (s != TWI_OK) return s;
         }
         EngineLaunch L;
-        for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
+        for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeBackward}) {
             L.njobs = 0;
             long long nctas = 0;
             for (Request& R : active) {
@@ -212,11 +217,12 @@ int twi_engine_create(int order, int exact, int rows_per_warp, int max_requests,
     E->order = order;
     E->exact = exact != 0;
     E->shape = LaunchShape{rows_per_warp == 8 || rows_per_warp == 2 ? rows_per_warp : 4, 4};
+    E->shape_back = LaunchShape{backward_rows(rows_per_warp), 4};
     E->max_requests = max_requests;
     size_t off = 0;
     auto take = [&](size_t b) { size_t o = off; off = (off + b + 255) & ~size_t(255); return o; };
-    E->off_tmaps = take((size_t)max_requests * 3 * sizeof(CUtensorMap));
-    E->off_tmpl = take((size_t)max_requests * 3 * sizeof(MultiJob));
+    E->off_tmaps = take((size_t)max_requests * kMapsPerPlan * sizeof(CUtensorMap));
+    E->off_tmpl = take((size_t)max_requests * twi_engine::kModes * sizeof(MultiJob));
     E->total = off;
     for (int i = max_requests - 1; i >= 0; --i) E->free_slots.push_back(i);
     *out = E;
@@ -251,7 +257,8 @@ int twi_engine_submit(twi_engine* E, twi_plan* plan, int kind, const float* obse
                       long long tag) {
     if (!E || !plan) return efail(TWI_ERR_INVALID, "null argument");
     if (kind != 0 && kind != 1) return efail(TWI_ERR_INVALID, "kind must be 0 (forward) or 1 (gradient)");
-    int s = plan_check_compatible(plan, kind, E->order, E->exact, E->shape.rows_per_warp);
+    int s = plan_check_compatible(plan, kind, E->order, E->exact, E->shape.rows_per_warp,
+                                  E->shape_back.rows_per_warp);
     if (s != TWI_OK) return s;
     twi_engine::Request R;
     R.plan = plan;

@@ -110,18 +110,40 @@ struct StepDyn {
     int cur_base, cur_stride;
     int next_base, next_stride;
     int virt_base;
+    int lprev_base, lprev_stride;   // kModeBackward: the adjoint field's slots
+    int lcur_base, lcur_stride;
+    int lnext_base, lnext_stride;
 };
 
 __host__ __device__ inline StepDyn dyn_of(const StepArgs& a) {
     return StepDyn{a.it, a.prev_base, a.prev_stride, a.cur_base, a.cur_stride,
-                   a.next_base, a.next_stride, a.virt_base};
+                   a.next_base, a.next_stride, a.virt_base,
+                   a.lprev_base, a.lprev_stride, a.lcur_base, a.lcur_stride,
+                   a.lnext_base, a.lnext_stride};
 }
+
+// The per-step part of `d` written into `a`.
+__host__ __device__ inline void apply_dyn(StepArgs& a, const StepDyn& d) {
+    a.it = d.it;
+    a.prev_base = d.prev_base, a.prev_stride = d.prev_stride;
+    a.cur_base = d.cur_base, a.cur_stride = d.cur_stride;
+    a.next_base = d.next_base, a.next_stride = d.next_stride;
+    a.virt_base = d.virt_base;
+    a.lprev_base = d.lprev_base, a.lprev_stride = d.lprev_stride;
+    a.lcur_base = d.lcur_base, a.lcur_stride = d.lcur_stride;
+    a.lnext_base = d.lnext_base, a.lnext_stride = d.lnext_stride;
+}
+
+// Tensor maps per plan in the device tables of batches and the engine: the
+// plan's u^n box, u^{n-1} box and velocity box at its main tile height, then
+// the same three at the tile height of its adjoint-type launches.
+constexpr int kMapsPerPlan = 6;
 
 // One job of a multi-plan launch (device memory, 64-byte aligned).
 struct alignas(64) MultiJob {
     StepArgs a;
     int cta_begin;   // first CTA of this job in the launch
-    int plan;        // index of the plan's tensor maps (3 per plan)
+    int plan;        // index of the plan's tensor maps (kMapsPerPlan per plan)
     int nbc;         // boundary CTAs per shot group
     int ncta;        // CTAs of this job
 };
@@ -215,6 +237,14 @@ cudaError_t launch_step_persistent(int order, bool exact, StepMode mode, LaunchS
 cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape, const CUtensorMap& tm_c,
                                        const CUtensorMap& tm_p, const CUtensorMap& tm_vel,
                                        const PersistLaunch& P, cudaStream_t stream);
+// Fused backward steps of several plans in one launch (job table in device
+// memory) and engine launches of it; each job reads its plan's adjoint-height
+// tensor maps.
+cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
+                                  int njobs, long long nctas, const CUtensorMap* tmaps,
+                                  cudaStream_t stream);
+cudaError_t launch_backward_engine(int order, bool exact, LaunchShape shape, const EngineLaunch& L,
+                                   long long nctas, const CUtensorMap* tmaps, cudaStream_t stream);
 
 // Store n host integers into device memory through kernel parameters
 // (chunks of 2048), ordered on `stream` without a host synchronisation.

@@ -1061,11 +1061,16 @@ int twi_plan_destroy(twi_plan* P) {
 // plan operations used by the request engine (twi_engine.cu)
 // ---------------------------------------------------------------------------
 
-void plan_tensor_maps(const twi_plan* P, CUtensorMap out[3]) {
+void plan_tensor_maps(const twi_plan* P, CUtensorMap out[kMapsPerPlan]) {
+    const bool own_adj = P->gradient && P->rz_adj != P->rz;   // ta_* exist
     out[0] = P->tm_u2;
     out[1] = P->tm_u1;
     out[2] = P->tm_vel;
+    out[3] = own_adj ? P->ta_u2 : P->tm_u2;
+    out[4] = own_adj ? P->ta_u1 : P->tm_u1;
+    out[5] = own_adj ? P->ta_vel : P->tm_vel;
 }
+int plan_adjoint_rows(const twi_plan* P) { return P->rz_adj; }
 float* plan_gathers(const twi_plan* P) { return P->F(P->off_frd); }
 long long plan_gathers_elems(const twi_plan* P) {
     return (long long)P->p.nshots * P->p.nt * P->p.nx;
@@ -1078,15 +1083,20 @@ void plan_steps(const twi_plan* P, int kind, std::vector<TwiStep>& out, size_t* 
 int plan_gradient_prologue(const twi_plan* P, cudaStream_t st) { return P->gradient_prologue(st); }
 int plan_gradient_epilogue(const twi_plan* P, cudaStream_t st) { return P->gradient_epilogue(st); }
 void plan_mark_done(twi_plan* P, int kind) { P->have_ckpt = kind == 1; }
-int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp) {
+int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp,
+                          int back_rows) {
     if (!P->ws) return fail(TWI_ERR_STATE, "bind the plan before submitting it");
     if (kind == 1 && !P->gradient) return fail(TWI_ERR_STATE, "a forward-only plan cannot take a gradient request");
     if (P->exa) return fail(TWI_ERR_INVALID, "excitation-amplitude plans run through twi_forward/twi_gradient only");
-    if (P->recon) return fail(TWI_ERR_INVALID, "reverse-reconstruction plans run through twi_forward/twi_gradient only");
+    if (P->recon && !P->fused_back)
+        return fail(TWI_ERR_INVALID, "plans with separate rebuild and adjoint launches (reconstruct = 2) run "
+                                     "through twi_forward/twi_gradient only");
     if (!P->have_shots || !P->have_model) return fail(TWI_ERR_STATE, "set shots and model first");
     if (P->p.order != order || (P->p.exact != 0) != exact ||
         default_shape(P->rz).rows_per_warp != rows_per_warp)
         return fail(TWI_ERR_INVALID, "plan order/arithmetic/rows_per_warp differ from the engine's");
+    if (P->fused_back && kind == 1 && P->rz_adj != back_rows)
+        return fail(TWI_ERR_INVALID, "plan's backward rows per warp differ from the engine's");
     return TWI_OK;
 }
 
@@ -1099,6 +1109,7 @@ struct twi_batch {
     int order = 4;
     bool exact = true, use_graphs = true;
     LaunchShape shape{4, 4};
+    LaunchShape shape_back{2, 4};   // fused backward launches of boundary-saving plans
     struct Launch {
         StepMode mode;
         size_t job0;   // first job in the phase's table
@@ -1144,14 +1155,15 @@ struct twi_batch {
         launches[phase].clear();
         const size_t T = max_steps(per);
         for (size_t t = 0; t < T; ++t) {
-            for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint}) {
+            for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeBackward}) {
                 Launch L{m, jobs.size(), 0, 0};
                 for (size_t i = 0; i < plans.size(); ++i) {
                     if (t >= per[i].size() || per[i][t].mode != m) continue;
                     MultiJob J{};
                     J.a = per[i][t].a;
                     J.plan = (int)i;
-                    J.ncta = step_ctas(order, shape, J.a, &J.nbc);
+                    J.ncta = m == kModeBackward ? backward_ctas(order, shape_back.rows_per_warp, J.a, &J.nbc)
+                                                : step_ctas(order, shape, J.a, &J.nbc);
                     if (J.ncta <= 0) return fail(TWI_ERR_INVALID, "batch launch too large");
                     J.cta_begin = (int)L.nctas;
                     L.nctas += J.ncta;
@@ -1174,8 +1186,9 @@ struct twi_batch {
         const MultiJob* base = reinterpret_cast<const MultiJob*>(ws + off_jobs[phase]);
         const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
         for (const Launch& L : launches[phase]) {
-            cudaError_t e = launch_step_multi(order, exact, L.mode, shape, base + L.job0, L.njobs,
-                                              L.nctas, tm, st);
+            cudaError_t e = L.mode == kModeBackward
+                ? launch_backward_multi(order, exact, shape_back, base + L.job0, L.njobs, L.nctas, tm, st)
+                : launch_step_multi(order, exact, L.mode, shape, base + L.job0, L.njobs, L.nctas, tm, st);
             if (e != cudaSuccess)
                 return fail(TWI_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
         }
@@ -1224,14 +1237,16 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
             B->exact = P->p.exact != 0;
             B->use_graphs = P->p.use_graphs != 0;
             B->shape = default_shape(P->rz);
+            B->shape_back = LaunchShape{P->rz_adj, 4};
         }
-        if (P->exa || P->recon) {
+        if (P->exa || (P->recon && !P->fused_back)) {
             delete B;
-            return fail(TWI_ERR_INVALID, "excitation-amplitude and reverse-reconstruction plans run through "
-                                         "twi_forward/twi_gradient only");
+            return fail(TWI_ERR_INVALID, "excitation-amplitude plans and plans with separate rebuild and adjoint "
+                                         "launches (reconstruct = 2) run through twi_forward/twi_gradient only");
         }
         if (P->p.order != B->order || (P->p.exact != 0) != B->exact ||
-                   default_shape(P->rz).rows_per_warp != B->shape.rows_per_warp) {
+                   default_shape(P->rz).rows_per_warp != B->shape.rows_per_warp ||
+                   (P->fused_back && P->rz_adj != B->shape_back.rows_per_warp)) {
             delete B;
             return fail(TWI_ERR_INVALID, "plans of a batch must share order, arithmetic and rows_per_warp");
         }
@@ -1240,11 +1255,11 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
     for (twi_plan* P : B->plans) {
         B->njobs[0] += P->p.nt;
         B->njobs[1] += P->p.nt;
-        B->njobs[2] += 2 * (size_t)P->p.nt;
+        B->njobs[2] += (P->fused_back ? 1 : 2) * (size_t)P->p.nt;   // fused backward: one job per step
     }
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
-    B->off_tmaps = take(B->plans.size() * 3 * sizeof(CUtensorMap));
+    B->off_tmaps = take(B->plans.size() * kMapsPerPlan * sizeof(CUtensorMap));
     for (int ph = 0; ph < 3; ++ph) B->off_jobs[ph] = take(B->njobs[ph] * sizeof(MultiJob));
     B->total = off;
     *out = B;
@@ -1266,12 +1281,8 @@ int twi_batch_bind(twi_batch* B, void* workspace, size_t bytes) {
         if (!P->ws) return fail(TWI_ERR_STATE, "bind every plan before its batch");
     B->drop_graphs();
     B->ws = static_cast<char*>(workspace);
-    std::vector<CUtensorMap> tm;
-    for (twi_plan* P : B->plans) {
-        tm.push_back(P->tm_u2);
-        tm.push_back(P->tm_u1);
-        tm.push_back(P->tm_vel);
-    }
+    std::vector<CUtensorMap> tm(B->plans.size() * kMapsPerPlan);
+    for (size_t i = 0; i < B->plans.size(); ++i) plan_tensor_maps(B->plans[i], &tm[i * kMapsPerPlan]);
     TWI_CUDA(cudaMemcpy(B->ws + B->off_tmaps, tm.data(), tm.size() * sizeof(CUtensorMap),
                         cudaMemcpyHostToDevice));
     for (bool& b : B->built) b = false;

@@ -37,8 +37,16 @@ void set_last_error(const std::string& msg);
 
 }  // namespace twi
 
-// Tensor maps of a bound plan: u^n box, u^{n-1} box, velocity box.
-void plan_tensor_maps(const twi_plan* P, CUtensorMap out[3]);
+// Tensor maps of a bound plan (kMapsPerPlan): u^n box, u^{n-1} box, velocity
+// box at the main tile height, then the same at the adjoint-type launches'
+// height; and that height in rows per warp.
+void plan_tensor_maps(const twi_plan* P, CUtensorMap out[twi::kMapsPerPlan]);
+int plan_adjoint_rows(const twi_plan* P);
+// Rows per warp of fused backward launches for an engine or plan created with
+// `rows_per_warp` (0 = choose): 2 unless 4 is asked for explicitly.
+inline int backward_rows(int rows_per_warp) {
+    return rows_per_warp == 4 || rows_per_warp == 8 ? 4 : 2;
+}
 // The gathers / residual region and its element count.
 float* plan_gathers(const twi_plan* P);
 long long plan_gathers_elems(const twi_plan* P);
@@ -48,4 +56,6 @@ void plan_steps(const twi_plan* P, int kind, std::vector<twi::TwiStep>& out, siz
 int plan_gradient_prologue(const twi_plan* P, cudaStream_t st);
 int plan_gradient_epilogue(const twi_plan* P, cudaStream_t st);
 void plan_mark_done(twi_plan* P, int kind);
-int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp);
+// rows_per_warp: the engine's tile height; back_rows: its fused backward's.
+int plan_check_compatible(const twi_plan* P, int kind, int order, bool exact, int rows_per_warp,
+                          int back_rows);

@@ -600,16 +600,6 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     }
 }
 
-// Copy one job's arguments into shared memory (all threads take part; the
-// body's first barrier orders the copy before any use).
-__device__ __forceinline__ void copy_args(StepArgs& dst, const StepArgs& src) {
-    static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied in 4-byte words");
-    const int* s = reinterpret_cast<const int*>(&src);
-    int* d = reinterpret_cast<int*>(&dst);
-    for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / 4); i += blockDim.x) d[i] = s[i];
-    __syncthreads();
-}
-
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
 step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ CUtensorMap tm_u1,
@@ -621,7 +611,7 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 
 // Several plans (different grids, shots, time indices) in one launch: CTA
 // ranges of the jobs are contiguous and ascending in jobs[].cta_begin; the
-// tensor maps of plan p are tmaps[3p .. 3p+2].
+// main-height tensor maps of plan p are tmaps[6p .. 6p+2].
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
 step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
@@ -633,7 +623,7 @@ step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
         else hi = mid - 1;
     }
     const MultiJob& J = jobs[lo];
-    const CUtensorMap* tm = tmaps + 3 * J.plan;
+    const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan;
     // Read through a pointer into global memory, the arguments would have to
     // be re-read from there after the kernel's own global stores.  The
     // forward step copies them into registers; the recompute and adjoint
@@ -677,7 +667,7 @@ step_kernel_engine(const __grid_constant__ EngineLaunch L, const CUtensorMap* __
         else hi = mid - 1;
     }
     const MultiJob& J = *L.tmpl[lo];
-    const CUtensorMap* tm = tmaps + 3 * J.plan;
+    const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan;
     if constexpr (MODE == kModeForward) {   // arguments copied as in step_kernel_multi
         const StepArgs a = J.a;
         step_body<ORDER, EXACT, MODE, RZ, WZ>(tm, tm + 1, tm + 2, a, L.dyn[lo], J.nbc,

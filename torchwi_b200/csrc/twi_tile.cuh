@@ -54,4 +54,26 @@ __device__ __forceinline__ void boundary_cell_at(int idx, int dimx, int dimz, in
     }
 }
 
+// Copy one job's arguments into shared memory (all threads take part, and
+// the barrier at the end orders the copy before any use).
+__device__ __forceinline__ void copy_args(StepArgs& dst, const StepArgs& src) {
+    static_assert(sizeof(StepArgs) % 4 == 0, "StepArgs is copied in 4-byte words");
+    const int* s = reinterpret_cast<const int*>(&src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(StepArgs) / 4); i += blockDim.x) d[i] = s[i];
+    __syncthreads();
+}
+
+// Index of the last job whose first CTA is at or before `cta` (begin[] ascending).
+template <typename Begin>
+__device__ __forceinline__ int job_of(Begin begin, int njobs, int cta) {
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (begin(mid) <= cta) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 }  // namespace twi
