@@ -82,6 +82,7 @@ struct twi_engine {
         int slot = -1;                  // tensor-map / template slot
         std::vector<TwiStep> steps;     // forward steps, then gradient steps
         int nbc[kModes] = {}, ncta[kModes] = {};   // per kernel mode
+        CUtensorMap tm[kMapsPerPlan];   // host copy of the plan's tensor maps
         size_t fwd_steps = 0, pos = 0;
         bool started = false;
     };
@@ -104,6 +105,7 @@ struct twi_engine {
             ENG_CUDA(cudaEventSynchronize(slot_events[R.slot]));
             SlotStage& S = staging[R.slot];
             plan_tensor_maps(R.plan, S.tm);
+            std::memcpy(R.tm, S.tm, sizeof(R.tm));
             bool seen[kModes] = {};
             for (const TwiStep& t : R.steps) {   // static arguments per kernel mode
                 const int m = static_cast<int>(t.mode);
@@ -165,6 +167,21 @@ struct twi_engine {
         for (StepMode m : {kModeForward, kModeRecompute, kModeAdjoint, kModeBackward}) {
             L.njobs = 0;
             long long nctas = 0;
+            // a mode with one job takes the single-plan kernel with the job's own
+            // arguments and tensor maps, exactly as the plan alone launches it
+            Request* only = nullptr;
+            int count = 0;
+            for (Request& R : active)
+                if (R.pos < R.steps.size() && R.steps[R.pos].mode == m) only = &R, ++count;
+            if (count == 1) {
+                const StepArgs& a = only->steps[only->pos].a;
+                cudaError_t e = m == kModeBackward
+                    ? launch_backward(order, exact, shape_back, only->tm[3], only->tm[4], only->tm[5], a, st)
+                    : launch_step(order, exact, m, shape, only->tm[0], only->tm[1], only->tm[2], a, st);
+                if (e != cudaSuccess)
+                    return efail(TWI_ERR_CUDA, std::string("engine launch: ") + cudaGetErrorString(e));
+                continue;
+            }
             for (Request& R : active) {
                 if (R.pos >= R.steps.size() || R.steps[R.pos].mode != m) continue;
                 if (L.njobs == kEngineMaxJobs) {   // full: launch and start another

@@ -281,7 +281,13 @@ class ShotPlan:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             try:
-                torch.cuda.synchronize(self.device)
+                # a caller that knows the plan's work has finished (an event
+                # after its last use) spares the device-wide wait
+                done = getattr(self, "_done", None)
+                if done is not None:
+                    done.synchronize()
+                else:
+                    torch.cuda.synchronize(self.device)
             except Exception:
                 pass
             self._lib.twi_plan_destroy(h)

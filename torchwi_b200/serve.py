@@ -165,6 +165,8 @@ class Server:
         self._parts: dict[int, list] = {}
         self._next = 0
         self.finished: list[Request] = []
+        # reported by the engine, results being copied out: (event, chunk, result)
+        self._completing: list = []
 
     def _options(self, req: Request) -> PlanOptions:
         return dataclasses.replace(self.options, forward_only=req.kind == "forward")
@@ -220,25 +222,40 @@ class Server:
             self.active_cells += ch.cells
 
     def poll(self, ticks=64) -> list[Request]:
-        """Admit what fits, advance the device, return requests that completed."""
+        """Admit what fits, advance the device, return requests that completed.
+
+        The stream is never drained: when the engine reports a request, its
+        result is copied out on the stream and an event marks the copy; the
+        request completes (and its plan and memory are released) once that
+        event has passed, while the other requests keep the GPU busy."""
         self._admit()
-        if not self.inflight:
-            return []
-        done_keys = self.engine.run(ticks)
-        if not done_keys:
-            return []
-        torch.cuda.current_stream(self.device).synchronize()
+        if self.inflight:
+            done_keys = self.engine.run(ticks)
+            stream = torch.cuda.current_stream(self.device)
+            for key in done_keys:
+                ch = self.inflight.pop(key)
+                res = (ch.plan.gathers if ch.req.kind == "forward" else ch.plan.grad).clone()
+                ev = torch.cuda.Event()
+                ev.record(stream)
+                self._completing.append((ev, ch, res))
+        elif self._completing:   # nothing left to advance: wait for the oldest copy
+            self._completing[0][0].synchronize()
+        return self._retire()
+
+    def _retire(self) -> list[Request]:
         now = time.perf_counter()
-        out = []
-        for key in done_keys:
-            ch = self.inflight.pop(key)
+        out, keep = [], []
+        for ev, ch, res in self._completing:
+            if not ev.query():
+                keep.append((ev, ch, res))
+                continue
             r = ch.req
-            res = (ch.plan.gathers if r.kind == "forward" else ch.plan.grad).clone()
             parts = self._parts[r.tag]
             idx = next(i for i, p in enumerate(parts) if p is None)
             parts[idx] = (ch.shots.start, res)
             self.used -= ch.footprint
             self.active_cells -= ch.cells
+            ch.plan._done = ev   # its work has finished: no device-wide wait on release
             ch.plan = None
             if all(p is not None for p in parts):
                 parts.sort(key=lambda t: t[0])
@@ -253,10 +270,11 @@ class Server:
                 del self._parts[r.tag]
                 self.finished.append(r)
                 out.append(r)
+        self._completing = keep
         return out
 
     def busy(self) -> bool:
-        return bool(self.queue or self.inflight)
+        return bool(self.queue or self.inflight or self._completing)
 
 
 def run_stream(server: Server, requests: list[Request], ticks=64) -> dict:
