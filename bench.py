@@ -588,7 +588,8 @@ def run_serve(args):
         srv.submit(warm[0])
         while srv.busy():
             srv.poll(64)
-        srv = Server(models, h=10.0, dt=1e-3, options=opts, max_requests=64, device=dev)
+        srv = Server(models, h=10.0, dt=1e-3, options=opts, max_requests=64, device=dev,
+                     policy=args.policy)
         reqs = mk()
         stats = run_stream(srv, reqs, ticks=args.ticks)
         svc = plain_service_times(models, mk(), 10.0, 1e-3, options=opts, device=dev)
@@ -604,6 +605,7 @@ def run_serve(args):
         del srv
         torch.cuda.empty_cache()
     print(json.dumps({"workload": "config5 serving stream", "requests_per_rate": args.requests,
+                      "policy": args.policy,
                       "adjoint_wavefield": "checkpoints" if args.checkpoints else "boundary saving, fused backward",
                       "max_shots": args.max_shots, "nt_range": [args.nt_min, args.nt_max],
                       "grids": [list(g) for g in synthetic.SERVE_GRIDS],
@@ -643,6 +645,9 @@ def main():
     ap.add_argument("--nt-min", type=int, default=2000)
     ap.add_argument("--nt-max", type=int, default=8000)
     ap.add_argument("--ticks", type=int, default=64)
+    ap.add_argument("--policy", default="fifo", choices=["fifo", "sjf"],
+                    help="serve: admission order (arrival order with small requests backfilled, "
+                         "or shortest first)")
     ap.add_argument("--workload", default="config2", choices=["config2", "config3", "config4", "serve"],
                     help="config2: the 64-shot gradient (default, the contract line); "
                          "config3: 256 shots, nt=6000 (with --checkpoints: a checkpoint every 50 steps); "

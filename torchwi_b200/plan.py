@@ -161,6 +161,8 @@ class ShotPlan:
         self.wavelet_per_shot = bool(wavelet_per_shot)
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
+        if self.device.index is None:   # "cuda" means the current device
+            self.device = torch.device("cuda", torch.cuda.current_device())
         self._lib = _capi.lib()
         prob = _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, self.options)
         self._h = ctypes.c_void_p()

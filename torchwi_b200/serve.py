@@ -136,16 +136,25 @@ def chunk_shots(nshots: int, footprint_of, budget: int) -> list[slice]:
 class Server:
     """Continuous-batching server over a resident model pool.
 
-    Admission: waiting chunks are taken shortest-job-first (estimated cell
-    updates) while (a) their plan footprints fit the HBM budget and (b) the
-    cell updates per time step of everything in flight stay below
-    `saturation_cells` -- roughly what fills the GPU -- so small requests are
-    batched together while a request that fills the GPU on its own does not
-    slow the others down.  There is always at least one request in flight."""
+    Admission (policy="fifo", the default): waiting chunks are admitted in
+    arrival order while (a) their plan footprints fit the HBM budget and (b)
+    the cell updates per time step of everything in flight stay below
+    `saturation_cells` -- roughly what fills the GPU; besides, any waiting
+    chunk of at most `backfill_cells` cell updates per step is admitted at
+    once (if it fits the budget) and runs alongside whatever is in flight,
+    so a small request does not wait behind a large one and a large one
+    keeps its place in line.  policy="sjf" takes the shortest waiting chunk
+    first instead (lower median latency, a longer tail for early large
+    requests).  There is always at least one request in flight."""
 
     def __init__(self, models: dict, h: float, dt: float, order=4, hbm_budget: int | None = None,
                  options: PlanOptions | None = None, max_requests=64, device=None,
-                 saturation_cells: int = 8_000_000):
+                 saturation_cells: int = 8_000_000, backfill_cells: int = 2_000_000,
+                 policy: str = "fifo"):
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy must be 'fifo' or 'sjf'")
+        self.policy = policy
+        self.backfill_cells = int(backfill_cells)
         self.device = torch.device(device) if device is not None else torch.device(
             "cuda", torch.cuda.current_device())
         self.models = {k: v.to(self.device, torch.float32) for k, v in models.items()}
@@ -188,13 +197,23 @@ class Server:
                                      work=cells * req.nt * (3.0 if req.kind == "gradient" else 1.0)))
 
     def _next_chunk(self):
-        self.queue.sort(key=lambda c: c.work)
-        for i, ch in enumerate(self.queue):
-            if self.used + ch.footprint > self.budget:
-                continue
-            if self.inflight and self.active_cells + ch.cells > self.saturation_cells:
-                continue
-            return self.queue.pop(i)
+        """The next chunk to admit, or None.  The queue is kept in arrival
+        order (chunks of one request stay together)."""
+        fits = lambda ch: self.used + ch.footprint <= self.budget  # noqa: E731
+        if self.policy == "sjf":
+            order = sorted(range(len(self.queue)), key=lambda i: self.queue[i].work)
+            for i in order:
+                ch = self.queue[i]
+                if fits(ch) and not (self.inflight and self.active_cells + ch.cells > self.saturation_cells):
+                    return self.queue.pop(i)
+            return None
+        if self.queue:   # the head of the line, when the GPU has room for it
+            ch = self.queue[0]
+            if fits(ch) and not (self.inflight and self.active_cells + ch.cells > self.saturation_cells):
+                return self.queue.pop(0)
+        for i, ch in enumerate(self.queue):   # small chunks run alongside
+            if ch.cells <= self.backfill_cells and fits(ch):
+                return self.queue.pop(i)
         return None
 
     def _admit(self):
