@@ -205,6 +205,13 @@ int twi_forward(twi_plan* plan, int save_checkpoints, void* stream);
  * laid out like `gathers`; `misfit` is one device double.  Follow with
  * twi_gradient. */
 int twi_forward_residual(twi_plan* plan, const float* observed, double* misfit, void* stream);
+/* The residual and misfit of twi_forward_residual, formed after a
+ * twi_forward(plan, 1, stream) from the gathers it left: resid = gathers -
+ * observed in place (the same bits) and *misfit as there.  Lets a caller
+ * bring `observed` to the device while the forward pass runs (no
+ * counterpart in the reference, whose driver forms the residual with torch,
+ * examples/time/inv_torch.py:133-136).  Follow with twi_gradient. */
+int twi_residual(twi_plan* plan, const float* observed, double* misfit, void* stream);
 /* Adjoint pass for all shots from the `resid` region: recomputes the
  * forward field segment by segment from the checkpoints and writes the
  * shot-summed velocity gradient to `grad`. */

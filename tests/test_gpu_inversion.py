@@ -115,3 +115,33 @@ def test_inversion_reduces_misfit_in_chunks():
                     hbm_budget=6 * 2 ** 20)
     hist = inv.run(6)
     assert hist[-1] < 0.7 * hist[0], hist
+
+
+@pytest.mark.parametrize("reconstruct", [False, True])
+def test_residual_after_forward_equals_forward_residual(reconstruct):
+    """twi_residual (residual + misfit formed after a saving forward pass, so
+    the observed gathers can be uploaded during the pass) gives the bits of
+    the fused twi_forward_residual: residual, misfit and gradient."""
+    s = synthetic.small_case(nx=90, nz=40, nt=160, order=4, nshots=5, seed=31)
+    dev = torch.device("cuda")
+    p = ShotPlan(s.nx, s.nz, s.h, s.dt, s.nt, 4, nshots=s.nshots,
+                 options=PlanOptions(reconstruct=reconstruct), device=dev)
+    p.set_wavelet(torch.from_numpy(s.w))
+    p.set_shots(s.sx, s.sy, s.ry)
+    p.set_model(torch.from_numpy(s.vel).to(dev))
+    obs = p.forward(save_checkpoints=False).clone()
+    out = []
+    for fused in (True, False):
+        p.set_model(torch.from_numpy(s.vel_start).to(dev))
+        if fused:
+            m = p.forward_residual(obs)
+        else:
+            p.forward(save_checkpoints=True)
+            m = p.residual(obs)
+        r = p.resid.clone()
+        g = p.gradient(None).clone()
+        p.check()
+        out.append((m.item(), r.cpu().numpy(), g.cpu().numpy()))
+    assert out[0][0] == out[1][0] and out[0][0] > 0
+    assert np.array_equal(out[0][1].view(np.int32), out[1][1].view(np.int32))
+    assert np.array_equal(out[0][2].view(np.int32), out[1][2].view(np.int32))

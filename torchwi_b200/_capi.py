@@ -74,6 +74,7 @@ SIGNATURES = {
     "twi_plan_set_model": [_vp, _vp],
     "twi_forward": [_vp, _i, _vp],
     "twi_forward_residual": [_vp, _vp, _vp, _vp],
+    "twi_residual": [_vp, _vp, _vp, _vp],
     "twi_gradient": [_vp, _vp],
     "twi_plan_check": [_vp, _vp],
     "twi_plan_profile": [_vp, _i, _i, ctypes.POINTER(ctypes.c_float), _vp],

@@ -47,12 +47,6 @@ int efail(int code, const std::string& msg) {
             return efail(TWI_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-__global__ void residual_kernel(float* __restrict__ frd, const float* __restrict__ obs, long long n) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        frd[i] = frd[i] - obs[i];
-}
-
 }  // namespace
 
 using namespace twi;
@@ -140,8 +134,7 @@ struct twi_engine {
             if (R.observed) {   // NULL observed gathers: zero data, residual = gathers
                 float* frd = plan_gathers(R.plan);
                 const long long n = plan_gathers_elems(R.plan);
-                residual_kernel<<<592, 256, 0, st>>>(frd, R.observed, n);
-                ENG_CUDA(cudaGetLastError());
+                ENG_CUDA(launch_residual(frd, R.observed, n, st));
             }
             int s = plan_gradient_prologue(R.plan, st);
             if (s != TWI_OK) return s;

@@ -263,6 +263,8 @@ cudaError_t launch_pad_model(const float* vel_user, float* vpad, int nx, int nz,
 constexpr int kMisfitBlocks = 592;
 cudaError_t launch_misfit(const float* r, long long n, double* partial, double* misfit,
                           cudaStream_t stream);
+// frd[i] = frd[i] - obs[i] for n samples (one FP32 subtraction each).
+cudaError_t launch_residual(float* frd, const float* obs, long long n, cudaStream_t stream);
 
 cudaError_t launch_reduce_grad(const float* acc, const float* acc_comp, int nacc,
                                long long slot_elems, int pitch, int ne, int nx, int nz,

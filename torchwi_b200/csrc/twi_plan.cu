@@ -844,6 +844,20 @@ int twi_forward_residual(twi_plan* P, const float* observed, double* misfit, voi
     return TWI_OK;
 }
 
+int twi_residual(twi_plan* P, const float* observed, double* misfit, void* stream) {
+    if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
+    if (!P->have_ckpt)
+        return fail(TWI_ERR_STATE, "twi_residual needs a preceding twi_forward(save_checkpoints=1)");
+    if (!observed || !misfit) return fail(TWI_ERR_INVALID, "observed and misfit must not be null");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long n = (long long)P->p.nshots * P->p.nt * P->p.nx;
+    cudaError_t e = launch_residual(P->F(P->off_frd), observed, n, st);
+    if (e == cudaSuccess)
+        e = launch_misfit(P->F(P->off_frd), n, reinterpret_cast<double*>(P->ws + P->off_mpart), misfit, st);
+    if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("residual: ") + cudaGetErrorString(e));
+    return TWI_OK;
+}
+
 int twi_gradient(twi_plan* P, void* stream) {
     if (!P || !P->ws) return fail(TWI_ERR_STATE, "plan has no workspace");
     if (!P->have_ckpt)

@@ -890,6 +890,14 @@ __global__ void reduce_grad_kernel(const float* __restrict__ acc, const float* _
     }
 }
 
+// residual = modelled - observed in place, one FP32 subtraction per sample
+// (the bits of the forward kernel's fused residual and of torch's frd - obs).
+__global__ void residual_kernel(float* __restrict__ frd, const float* __restrict__ obs, long long n) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        frd[i] = __fsub_rn(frd[i], obs[i]);
+}
+
 // Misfit, pass 1: a fixed grid of kMisfitBlocks blocks; block b sums, in
 // FP64, the squares of the float4 groups b, b + grid, ... (thread-strided,
 // then a fixed tree), so the result does not depend on timing.
@@ -938,6 +946,11 @@ cudaError_t launch_misfit(const float* r, long long n, double* partial, double* 
     if (reinterpret_cast<uintptr_t>(r) % 16 != 0) return cudaErrorMisalignedAddress;
     misfit_partial_kernel<<<kMisfitBlocks, 256, 0, stream>>>(r, n, partial);
     misfit_final_kernel<<<1, 256, 0, stream>>>(partial, kMisfitBlocks, misfit);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual(float* frd, const float* obs, long long n, cudaStream_t stream) {
+    residual_kernel<<<kMisfitBlocks, 256, 0, stream>>>(frd, obs, n);
     return cudaGetLastError();
 }
 

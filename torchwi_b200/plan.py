@@ -246,6 +246,25 @@ class ShotPlan:
         self._keep_obs = observed   # the captured graph reads it
         return misfit
 
+    def residual(self, observed: torch.Tensor, misfit: torch.Tensor | None = None) -> torch.Tensor:
+        """After forward(save_checkpoints=True): turn the gathers into the
+        residual modelled - observed in place and return the misfit
+        0.5*sum(residual^2) (0-d float64 on the device), the same bits as
+        forward_residual.  `observed` only has to be on the device when the
+        forward pass ends, so its upload can overlap the pass.  Follow with
+        gradient(None)."""
+        if observed.device != self.device or observed.dtype != torch.float32 or not observed.is_contiguous():
+            raise _capi.TwiInvalid(_capi.TWI_ERR_INVALID,
+                                   "observed must be a contiguous float32 tensor on the plan's device")
+        if observed.numel() != self.gathers.numel():
+            raise _capi.TwiInvalid(_capi.TWI_ERR_INVALID, f"observed must hold {tuple(self.gathers.shape)} samples")
+        if misfit is None:
+            misfit = torch.empty((), dtype=torch.float64, device=self.device)
+        with torch.cuda.device(self.device):
+            check(self._lib.twi_residual(self._h, ctypes.c_void_p(observed.data_ptr()),
+                                         ctypes.c_void_p(misfit.data_ptr()), _stream_handle()))
+        return misfit
+
     def gradient(self, resid: torch.Tensor | None = None) -> torch.Tensor:
         """Adjoint pass from `resid` [nshots, nt, nx] (already in the resid
         region when None); returns the (nx, nz) gradient view."""
