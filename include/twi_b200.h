@@ -47,8 +47,10 @@ const char* twi_last_error(void);
  * pointers except `w`, which may be host or device memory (the reference
  * keeps it on the host).  Semantics are those of the reference's CPU
  * propagator (unpadded grid, Keys on left/right/bottom, free top), computed
- * on the GPU with bit-identical FP32 results.  u1/u2/u3 are accepted for
- * signature compatibility and left untouched; scratch is taken with
+ * on the GPU with bit-identical FP32 results.  u1/u2/u3 ([dimy][dimx]
+ * device arrays, as the reference's work arrays) receive on return the last
+ * three wavefields, arranged as the reference's rotating pointers leave
+ * them; passing NULL for any of them skips that.  Scratch is taken with
  * cudaMallocAsync on `stream` and released before return.
  * ------------------------------------------------------------------------ */
 

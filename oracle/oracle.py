@@ -187,8 +187,9 @@ def twio_exa_backward(exa, iexa, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
     return grad
 
 
-def ref_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
-    """The reference's compiled c_fdm_forward.  Returns (frd, virt)."""
+def ref_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry, return_fields=False):
+    """The reference's compiled c_fdm_forward.  Returns (frd, virt), and with
+    return_fields the three work arrays u1, u2, u3 as the call left them."""
     lib = _load(_REF_SO)
     vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel().copy()
     w = np.ascontiguousarray(w, dtype=np.float32).ravel().copy()
@@ -198,10 +199,10 @@ def ref_forward(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
     u = [np.zeros(dimxy, dtype=np.float32) for _ in range(3)]
     lib.ref_fdm_forward(_ptr(frd), _ptr(virt), *(_ptr(a) for a in u), _ptr(vpad),
                         _ptr(w), order, dimx, dimy, nt, h, dt, sx, sy, ry)
-    return frd, virt
+    return (frd, virt, u) if return_fields else (frd, virt)
 
 
-def ref_forward_only(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
+def ref_forward_only(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry, return_fields=False):
     lib = _load(_REF_SO)
     vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel().copy()
     w = np.ascontiguousarray(w, dtype=np.float32).ravel().copy()
@@ -210,10 +211,10 @@ def ref_forward_only(vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
     u = [np.zeros(dimxy, dtype=np.float32) for _ in range(3)]
     lib.ref_fdm_forward_only(_ptr(frd), *(_ptr(a) for a in u), _ptr(vpad),
                              _ptr(w), order, dimx, dimy, nt, h, dt, sx, sy, ry)
-    return frd
+    return (frd, u) if return_fields else frd
 
 
-def ref_backward(virt, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
+def ref_backward(virt, vpad, resid, order, dimx, dimy, nt, h, dt, ry, return_fields=False):
     lib = _load(_REF_SO)
     virt = np.ascontiguousarray(virt, dtype=np.float32)
     vpad = np.ascontiguousarray(vpad, dtype=np.float32).ravel().copy()
@@ -223,7 +224,7 @@ def ref_backward(virt, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
     u = [np.zeros(dimxy, dtype=np.float32) for _ in range(3)]
     lib.ref_fdm_backward(_ptr(grad), _ptr(virt), *(_ptr(a) for a in u), _ptr(vpad),
                          _ptr(resid), order, dimx, dimy, nt, h, dt, ry)
-    return grad
+    return (grad, u) if return_fields else grad
 
 
 # ----------------------------------------------------------------------------

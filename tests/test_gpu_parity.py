@@ -76,6 +76,42 @@ def test_native_forward_backward_bitexact(order, shape):
     assert bits_equal(frd2.cpu().numpy().reshape(nt, nx), f_or)
 
 
+@pytest.mark.parametrize("order,nt", [(4, 150), (2, 97), (8, 121), (4, 2)])
+def test_native_work_arrays_left_like_the_reference(order, nt):
+    """The reference's propagator leaves its last three wavefields in the
+    caller's u1/u2/u3 (rotating pointers, propagator_cpu.cpp:57-78,
+    129-150); the drop-in entry points leave the same bits there, for the
+    forward, forward-only and adjoint passes (nt = 2: one array stays zero)."""
+    if not O.have_ref():
+        pytest.skip("the reference's CPU propagator (oracle/_ref) is not built")
+    nx, nz = 45, 27
+    s = synthetic.small_case(nx=nx, nz=nz, nt=nt, order=order, nshots=1, seed=order + nt)
+    dimx, dimy = nx + order, nz + order
+    vpad = O.pad_model(s.vel, order)
+    args = (order, dimx, dimy, nt, s.h, s.dt, s.sx[0], s.sy[0], s.ry[0])
+    f_ref, v_ref, u_ref = O.oracle.ref_forward(vpad, s.w, *args, return_fields=True)
+    dev = torch.device("cuda")
+    u = [torch.full((dimx * dimy,), 7.0, device=dev) for _ in range(3)]   # stale contents
+    vp = torch.from_numpy(vpad).to(dev)
+    frd = torch.zeros(nt * nx, device=dev)
+    virt = torch.zeros(nt * dimx * dimy, device=dev)
+    td2d_b200.forward(frd, virt, *u, vp, torch.from_numpy(s.w), *args)
+    for a, b in zip(u, u_ref):
+        assert bits_equal(a.cpu().numpy(), b)
+    _, u_fo = O.oracle.ref_forward_only(vpad, s.w, *args, return_fields=True)
+    u2 = [torch.full((dimx * dimy,), -3.0, device=dev) for _ in range(3)]
+    td2d_forward_b200.forward(torch.zeros_like(frd), *u2, vp, torch.from_numpy(s.w), *args)
+    for a, b in zip(u2, u_fo):
+        assert bits_equal(a.cpu().numpy(), b)
+    resid = (0.5 * f_ref).astype(np.float32)
+    _, u_bref = O.oracle.ref_backward(v_ref, vpad, resid, order, dimx, dimy, nt, s.h, s.dt, s.ry[0],
+                                      return_fields=True)
+    td2d_b200.backward(virt, *u, vp, torch.from_numpy(resid).to(dev).reshape(-1), order, dimx, dimy,
+                       nt, s.h, s.dt, s.ry[0])
+    for a, b in zip(u, u_bref):
+        assert bits_equal(a.cpu().numpy(), b)
+
+
 def test_native_rejects_bad_input():
     dev = torch.device("cuda")
     z = torch.zeros(64 * 44, device=dev)

@@ -1418,6 +1418,26 @@ struct RefRun {
         return TWI_OK;
     }
 
+    // Leave the last three wavefields in the caller's work arrays the way the
+    // reference's loop does (propagator_cpu.cpp:57-78, 129-150: its u3 is the
+    // output of each step and the three pointers rotate, so the field written
+    // in step c ends up in u3, u1, u2 for c % 3 = 0, 1, 2; arrays no step
+    // wrote keep the zeros the reference clears them to).  Step c wrote this
+    // run's slot rot_slot(c + 1).  Nothing happens when any pointer is null.
+    int mirror_fields(float* u1, float* u2, float* u3) const {
+        if (!u1 || !u2 || !u3) return TWI_OK;
+        float* buf[3] = {u3, u1, u2};
+        const size_t bytes = (size_t)dimx * dimz * 4;
+        for (float* b : buf) TWI_CUDA(cudaMemsetAsync(b, 0, bytes, st));
+        for (int c = nt - 3 < 0 ? 0 : nt - 3; c < nt; ++c) {
+            const long long k = (long long)c + 1;
+            const float* src = F(off_fields) + (long long)(1 + (int)(k % 3)) * slot_elems;
+            TWI_CUDA(cudaMemcpy2DAsync(buf[c % 3], (size_t)dimx * 4, src, (size_t)pitch * 4,
+                                       (size_t)dimx * 4, dimz, cudaMemcpyDeviceToDevice, st));
+        }
+        return TWI_OK;
+    }
+
     // read the error word, release scratch
     int finish(int status) {
         int err = 0;
@@ -1439,9 +1459,9 @@ struct RefRun {
 
 Slot rot_slot(long long k) { return k <= 0 ? Slot{0, 0} : Slot{1 + (int)(k % 3), 0}; }
 
-int ref_forward(float* frd, float* virt, const float* vel, const float* w, int order, int dimx,
-                int dimy, int nt, float h, float dt, float sx, float sy, float ry,
-                cudaStream_t st) {
+int ref_forward(float* frd, float* virt, float* u1, float* u2, float* u3, const float* vel,
+                const float* w, int order, int dimx, int dimy, int nt, float h, float dt, float sx,
+                float sy, float ry, cudaStream_t st) {
     if (!frd || !vel || !w) return fail(TWI_ERR_INVALID, "null array");
     RefRun R;
     int s = R.setup(order, dimx, dimy, nt, h, dt, false, st);
@@ -1469,6 +1489,7 @@ int ref_forward(float* frd, float* virt, const float* vel, const float* w, int o
             s = R.launch(virt ? kModeRecompute : kModeForward, a);
         }
     }
+    if (s == TWI_OK) s = R.mirror_fields(u1, u2, u3);
     return R.finish(s);
 }
 
@@ -1484,7 +1505,6 @@ extern "C" {
 int twi_fdm_exa_forward(float* frd, float* exa, short* iexa, float* u1, float* u2, float* u3,
                         const float* vel, const float* w, int order, int dimx, int dimy, int nt,
                         float h, float dt, float sx, float sy, float ry, void* stream) {
-    (void)u1, (void)u2, (void)u3;
     if (!frd || !exa || !iexa || !vel || !w) return fail(TWI_ERR_INVALID, "null array");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     RefRun R;
@@ -1516,13 +1536,13 @@ int twi_fdm_exa_forward(float* frd, float* exa, short* iexa, float* u1, float* u
                                (size_t)dimx * 2, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess))
             s = fail(TWI_ERR_CUDA, "excitation copy failed");
     }
+    if (s == TWI_OK) s = R.mirror_fields(u1, u2, u3);
     return R.finish(s);
 }
 
 int twi_fdm_exa_backward(float* grad, const float* exa, const short* iexa, float* u1, float* u2,
                          float* u3, const float* vel, const float* resid, int order, int dimx,
                          int dimy, int nt, float h, float dt, float ry, void* stream) {
-    (void)u1, (void)u2, (void)u3;
     if (!grad || !exa || !iexa || !vel || !resid) return fail(TWI_ERR_INVALID, "null array");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     RefRun R;
@@ -1565,30 +1585,28 @@ int twi_fdm_exa_backward(float* grad, const float* exa, const short* iexa, float
                               (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
             s = fail(TWI_ERR_CUDA, "gradient copy failed");
     }
+    if (s == TWI_OK) s = R.mirror_fields(u1, u2, u3);
     return R.finish(s);
 }
 
 int twi_fdm_forward(float* frd, float* virt, float* u1, float* u2, float* u3, const float* vel,
                     const float* w, int order, int dimx, int dimy, int nt, float h, float dt,
                     float sx, float sy, float ry, void* stream) {
-    (void)u1, (void)u2, (void)u3;
     if (!virt) return fail(TWI_ERR_INVALID, "virt must not be null (use twi_fdm_forward_only)");
-    return ref_forward(frd, virt, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
+    return ref_forward(frd, virt, u1, u2, u3, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
                        static_cast<cudaStream_t>(stream));
 }
 
 int twi_fdm_forward_only(float* frd, float* u1, float* u2, float* u3, const float* vel,
                          const float* w, int order, int dimx, int dimy, int nt, float h,
                          float dt, float sx, float sy, float ry, void* stream) {
-    (void)u1, (void)u2, (void)u3;
-    return ref_forward(frd, nullptr, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
+    return ref_forward(frd, nullptr, u1, u2, u3, vel, w, order, dimx, dimy, nt, h, dt, sx, sy, ry,
                        static_cast<cudaStream_t>(stream));
 }
 
 int twi_fdm_backward(float* grad, const float* virt, float* u1, float* u2, float* u3,
                      const float* vel, const float* resid, int order, int dimx, int dimy, int nt,
                      float h, float dt, float ry, void* stream) {
-    (void)u1, (void)u2, (void)u3;
     if (!grad || !virt || !vel || !resid) return fail(TWI_ERR_INVALID, "null array");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     RefRun R;
@@ -1628,6 +1646,7 @@ int twi_fdm_backward(float* grad, const float* virt, float* u1, float* u2, float
                               (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
             s = fail(TWI_ERR_CUDA, "gradient copy failed");
     }
+    if (s == TWI_OK) s = R.mirror_fields(u1, u2, u3);
     return R.finish(s);
 }
 

@@ -70,8 +70,8 @@ def forward(frd, virt, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, sx, sy
     if not w.is_contiguous():
         raise RuntimeError("w must be contiguous")
     w = w.to(torch.float32)
-    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((frd, "frd"),),
-                 history=((virt, "source_wavefield"),), w=w)
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (u1, "u1"), (u2, "u2"), (u3, "u3")),
+                 trace=((frd, "frd"),), history=((virt, "source_wavefield"),), w=w)
     with torch.cuda.device(frd.device):
         _run(_capi.lib().twi_fdm_forward(_ptr(frd), _ptr(virt), _ptr(u1), _ptr(u2), _ptr(u3),
                                          _ptr(vpad), _ptr(w), int(order), int(dimx), int(dimy),
@@ -83,8 +83,8 @@ def backward(virt, u1, u2, u3, vpad, resid, order, dimx, dimy, nt, h, dt, ry):
     for t, n in ((virt, "source_wavefield"), (u1, "u1"), (u2, "u2"), (u3, "u3"), (vpad, "vel"),
                  (resid, "resid")):
         _cuda_input(t, n)
-    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((resid, "resid"),),
-                 history=((virt, "source_wavefield"),))
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (u1, "u1"), (u2, "u2"), (u3, "u3")),
+                 trace=((resid, "resid"),), history=((virt, "source_wavefield"),))
     grad = torch.zeros_like(vpad)
     with torch.cuda.device(vpad.device):
         _run(_capi.lib().twi_fdm_backward(_ptr(grad), _ptr(virt), _ptr(u1), _ptr(u2), _ptr(u3),

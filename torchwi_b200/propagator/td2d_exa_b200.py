@@ -16,7 +16,8 @@ def forward(frd, exa, iexa, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, s
     if not iexa.is_cuda or iexa.dtype != torch.int16 or not iexa.is_contiguous():
         raise RuntimeError("iexa must be a contiguous int16 CUDA tensor")
     w = w.contiguous().to(torch.float32)
-    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (exa, "exa"), (iexa, "iexa")),
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (exa, "exa"), (iexa, "iexa"),
+                                             (u1, "u1"), (u2, "u2"), (u3, "u3")),
                  trace=((frd, "frd"),), w=w)
     with torch.cuda.device(frd.device):
         _run(_capi.lib().twi_fdm_exa_forward(_ptr(frd), _ptr(exa), _ptr(iexa), _ptr(u1), _ptr(u2),
@@ -30,7 +31,8 @@ def backward(exa, iexa, u1, u2, u3, vpad, resid, order, dimx, dimy, nt, h, dt, r
         _cuda_input(t, n)
     if not iexa.is_cuda or iexa.dtype != torch.int16 or not iexa.is_contiguous():
         raise RuntimeError("iexa must be a contiguous int16 CUDA tensor")
-    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (exa, "exa"), (iexa, "iexa")),
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (exa, "exa"), (iexa, "iexa"),
+                                             (u1, "u1"), (u2, "u2"), (u3, "u3")),
                  trace=((resid, "resid"),))
     grad = torch.zeros_like(vpad)
     with torch.cuda.device(vpad.device):

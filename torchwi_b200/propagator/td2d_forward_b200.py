@@ -15,7 +15,8 @@ def forward(frd, u1, u2, u3, vpad, w, order, dimx, dimy, nt, h, dt, sx, sy, ry):
     if not w.is_contiguous():
         raise RuntimeError("w must be contiguous")
     w = w.to(torch.float32)
-    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"),), trace=((frd, "frd"),), w=w)
+    _check_sizes(order, dimx, dimy, nt, grid=((vpad, "vel"), (u1, "u1"), (u2, "u2"), (u3, "u3")),
+                 trace=((frd, "frd"),), w=w)
     with torch.cuda.device(frd.device):
         _run(_capi.lib().twi_fdm_forward_only(_ptr(frd), _ptr(u1), _ptr(u2), _ptr(u3),
                                               _ptr(vpad), _ptr(w), int(order), int(dimx),
