@@ -524,7 +524,7 @@ cudaError_t back_one(const BackReq& q, cudaStream_t st) {
     if (pl) {
         int grid = 0;
         e = persistent_grid(backward_kernel_persistent<ORDER, EXACT, RZ, 4>, 128, S::BYTES,
-                            (long long)pl->nsteps * pl->ngroups * pl->per_group, &grid);
+                            (long long)pl->nsteps * pl->ngroups * pl->per_group, &grid, pl->max_ctas);
         if (e != cudaSuccess) return e;
         backward_kernel_persistent<ORDER, EXACT, RZ, 4><<<dim3((unsigned)grid), 128, S::BYTES, st>>>(*tc, *tp, *tv, *pl);
         return cudaGetLastError();

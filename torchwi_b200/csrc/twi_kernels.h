@@ -101,6 +101,7 @@ struct PersistLaunch {
     int nsteps, ngroups, per_group, nbc;
     unsigned* ticket;
     unsigned* count;
+    int max_ctas;   // 0: as many CTAs as fit the device; else at most this many
 };
 
 // The part of a time step's arguments that changes from step to step.

@@ -52,16 +52,20 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
 
 // Thread 0 only: wait until *count >= target.  False when the wait ran out
 // (bit 1 of *err raised) or another CTA reported an error.
+// Polls back off from 32 ns to 1 µs so that CTAs waiting on one counter do
+// not flood its L2 line.
 __device__ __forceinline__ bool wait_count(const unsigned* count, unsigned target, int* err) {
     const uint64_t t0 = globaltimer_ns();
+    unsigned ns = 32;
     for (uint32_t i = 0;; ++i) {
         if (ld_acquire_u32(count) >= target) return true;
         if (ld_volatile_s32(err) != 0) return false;
-        if ((i & 63u) == 63u && globaltimer_ns() - t0 > kWaitLimitNs) {
+        if ((i & 15u) == 15u && globaltimer_ns() - t0 > kWaitLimitNs) {
             atomicOr(err, 2);
             return false;
         }
-        __nanosleep(64);
+        __nanosleep(ns);
+        ns = ns < 1024 ? 2 * ns : 1024;
     }
 }
 
@@ -123,7 +127,8 @@ __device__ __forceinline__ void persistent_loop(const PersistLaunch& P, uint64_t
 // Host: the grid of a persistent launch -- as many CTAs as can be resident
 // at once on the current device (occupancy x SMs), at most one per work item.
 template <typename Kernel>
-cudaError_t persistent_grid(Kernel kernel, int threads, size_t smem_bytes, long long items, int* grid) {
+cudaError_t persistent_grid(Kernel kernel, int threads, size_t smem_bytes, long long items, int* grid,
+                            int max_ctas = 0) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -133,6 +138,7 @@ cudaError_t persistent_grid(Kernel kernel, int threads, size_t smem_bytes, long 
     if (items < 1) return cudaErrorInvalidConfiguration;
     long long g = (long long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
     if (g > items) g = items;
+    if (max_ctas > 0 && g > max_ctas) g = max_ctas;
     *grid = (int)g;
     return cudaSuccess;
 }

@@ -485,7 +485,7 @@ struct twi_plan {
         if (total <= 0 || ngroups < 1 || total % ngroups != 0)
             return fail(TWI_ERR_INVALID, "persistent launch too large");
         unsigned* cnt = reinterpret_cast<unsigned*>(ws + off_cnt);
-        const PersistLaunch L{dev, n, ngroups, total / ngroups, nbc, cnt, cnt + 1};
+        const PersistLaunch L{dev, n, ngroups, total / ngroups, nbc, cnt, cnt + 1, 0};
         TWI_CUDA(cudaMemsetAsync(cnt, 0, (size_t)(1 + ngroups) * sizeof(unsigned), st));
         const CUtensorMap& t2 = adj ? ta_u2 : tm_u2;
         const CUtensorMap& t1 = adj ? ta_u1 : tm_u1;
@@ -1344,7 +1344,9 @@ struct RefRun {
     float h, dt;
     char* scratch = nullptr;
     size_t off_vpad = 0, off_fields = 0, off_wav = 0, off_coords = 0, off_err = 0, off_acc = 0,
-           off_exa = 0, off_iexa = 0, total = 0;
+           off_exa = 0, off_iexa = 0, off_tab = 0, off_cnt = 0, total = 0;
+    std::vector<StepArgs> queued;
+    StepMode queued_mode = kModeForward;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
     cudaStream_t st = nullptr;
 
@@ -1372,6 +1374,8 @@ struct RefRun {
         off_wav = take((size_t)nt * 4);
         off_coords = take(3 * 4);
         off_err = take(4);
+        off_tab = take((size_t)nt * sizeof(StepArgs));   // the pass's steps, one persistent launch
+        off_cnt = take(2 * sizeof(unsigned));            // ticket + the one shot's counter
         total = off;
         void* p = nullptr;
         TWI_CUDA(cudaMallocAsync(&p, total, st));
@@ -1412,8 +1416,34 @@ struct RefRun {
         return a;
     }
 
-    int launch(StepMode mode, const StepArgs& a) const {
-        cudaError_t e = launch_step(order, true, mode, LaunchShape{4, 4}, tm_u2, tm_u1, tm_vel, a, st);
+    // Steps are queued and run by flush() as ONE persistent launch
+    // (twi_persist.cuh): a single shot's step is a few microseconds of work,
+    // so nt separate launches would be bound by launch latency.
+    int launch(StepMode mode, const StepArgs& a) {
+        if (!queued.empty() && queued_mode != mode) TWI_TRY(flush());
+        queued_mode = mode;
+        queued.push_back(a);
+        return TWI_OK;
+    }
+
+    int flush() {
+        if (queued.empty()) return TWI_OK;
+        if (queued.size() > (size_t)nt) return fail(TWI_ERR_STATE, "step table too small");
+        StepArgs* tab = reinterpret_cast<StepArgs*>(scratch + off_tab);
+        // pageable source: staged before the call returns
+        TWI_CUDA(cudaMemcpyAsync(tab, queued.data(), queued.size() * sizeof(StepArgs),
+                                 cudaMemcpyHostToDevice, st));
+        unsigned* cnt = reinterpret_cast<unsigned*>(scratch + off_cnt);
+        TWI_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned), st));
+        const LaunchShape sh{4, 4};
+        int nbc = 0;
+        const int per_step = step_ctas(order, sh, queued[0], &nbc);   // one shot: one group
+        if (per_step <= 0) return fail(TWI_ERR_INVALID, "launch too large");
+        // two steps' worth of CTAs: the next step's items are claimed while the
+        // current one finishes, without a device full of waiting CTAs
+        const PersistLaunch L{tab, (int)queued.size(), 1, per_step, nbc, cnt, cnt + 1, 2 * per_step};
+        cudaError_t e = launch_step_persistent(order, true, queued_mode, sh, tm_u2, tm_u1, tm_vel, L, st);
+        queued.clear();
         if (e != cudaSuccess) return fail(TWI_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
         return TWI_OK;
     }
@@ -1488,6 +1518,7 @@ int ref_forward(float* frd, float* virt, float* u1, float* u2, float* u3, const 
             a.virt_base = it;
             s = R.launch(virt ? kModeRecompute : kModeForward, a);
         }
+        if (s == TWI_OK) s = R.flush();
     }
     if (s == TWI_OK) s = R.mirror_fields(u1, u2, u3);
     return R.finish(s);
@@ -1529,6 +1560,7 @@ int twi_fdm_exa_forward(float* frd, float* exa, short* iexa, float* u1, float* u
             a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
             s = R.launch(kModeExaForward, a);
         }
+        if (s == TWI_OK) s = R.flush();
         if (s == TWI_OK &&
             (cudaMemcpy2DAsync(exa, (size_t)dimx * 4, R.F(R.off_exa), (size_t)R.pitch * 4,
                                (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
@@ -1580,6 +1612,7 @@ int twi_fdm_exa_backward(float* grad, const float* exa, const short* iexa, float
             a.prev_base = pv.base, a.cur_base = cu.base, a.next_base = nx_.base;
             s = R.launch(kModeAdjoint, a);
         }
+        if (s == TWI_OK) s = R.flush();
         if (s == TWI_OK &&
             cudaMemcpy2DAsync(grad, (size_t)dimx * 4, R.F(R.off_acc), (size_t)R.pitch * 4,
                               (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
@@ -1641,6 +1674,7 @@ int twi_fdm_backward(float* grad, const float* virt, float* u1, float* u2, float
             a.virt_base = it;
             s = R.launch(kModeAdjoint, a);
         }
+        if (s == TWI_OK) s = R.flush();
         if (s == TWI_OK &&
             cudaMemcpy2DAsync(grad, (size_t)dimx * 4, R.F(R.off_acc), (size_t)R.pitch * 4,
                               (size_t)dimx * 4, dimy, cudaMemcpyDeviceToDevice, st) != cudaSuccess)

@@ -751,7 +751,8 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     if (q.persist) {
         const long long items = (long long)q.persist->nsteps * q.persist->ngroups * q.persist->per_group;
         int grid = 0;
-        e = persistent_grid(step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>, WZ * 32, S::BYTES, items, &grid);
+        e = persistent_grid(step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>, WZ * 32, S::BYTES, items, &grid,
+                            q.persist->max_ctas);
         if (e != cudaSuccess) return e;
         step_kernel_persistent<ORDER, EXACT, MODE, RZ, WZ>
             <<<dim3((unsigned)grid), WZ * 32, S::BYTES, stream>>>(*q.t2, *q.t1, *q.tv, *q.persist);
