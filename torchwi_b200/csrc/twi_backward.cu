@@ -421,9 +421,9 @@ backward_kernel(const __grid_constant__ CUtensorMap tm_c, const __grid_constant_
 // that the body does not re-read them from global memory after its stores.
 template <int ORDER, bool EXACT, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, kBackCtasPerSm(RZ))
-backward_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
+backward_kernel_multi(const MultiJob* __restrict__ jobs, const int* __restrict__ begins, const int njobs,
                       const CUtensorMap* __restrict__ tmaps) {
-    const int lo = job_of([&](int i) { return jobs[i].cta_begin; }, njobs, (int)blockIdx.x);
+    const int lo = job_of([&](int i) { return begins[i]; }, njobs, (int)blockIdx.x);
     const MultiJob& J = jobs[lo];
     const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan + 3;
     __shared__ StepArgs a;
@@ -480,6 +480,7 @@ struct BackReq {
     const StepArgs* a = nullptr;
     const PersistLaunch* pl = nullptr;
     const MultiJob* jobs = nullptr;
+    const int* begins = nullptr;
     int njobs = 0;
     long long nctas = 0;
     const CUtensorMap* tmaps = nullptr;
@@ -518,7 +519,7 @@ cudaError_t back_one(const BackReq& q, cudaStream_t st) {
                 <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(*q.engine, q.tmaps);
         else
             backward_kernel_multi<ORDER, EXACT, RZ, 4>
-                <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(q.jobs, q.njobs, q.tmaps);
+                <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(q.jobs, q.begins, q.njobs, q.tmaps);
         return cudaGetLastError();
     }
     if (pl) {
@@ -584,11 +585,11 @@ cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape,
 }
 
 cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
-                                  int njobs, long long nctas, const CUtensorMap* tmaps,
-                                  cudaStream_t stream) {
+                                  const int* begins, int njobs, long long nctas,
+                                  const CUtensorMap* tmaps, cudaStream_t stream) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
     BackReq q;
-    q.jobs = jobs, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    q.jobs = jobs, q.begins = begins, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
     return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
 }
 

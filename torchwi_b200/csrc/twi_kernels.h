@@ -176,9 +176,10 @@ cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
 // CTAs a single-plan launch of `a` uses, and its boundary CTAs per shot group.
 int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc);
 
-// One launch covering several jobs (tensor maps in device memory).
+// One launch covering several jobs (tensor maps in device memory);
+// begins[i] = jobs[i].cta_begin, ascending.
 cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
-                              const MultiJob* jobs, int njobs, long long nctas,
+                              const MultiJob* jobs, const int* begins, int njobs, long long nctas,
                               const CUtensorMap* tmaps, cudaStream_t stream);
 
 // One engine launch (job entries in device memory, index in parameters).
@@ -242,8 +243,8 @@ cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape,
 // memory) and engine launches of it; each job reads its plan's adjoint-height
 // tensor maps.
 cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
-                                  int njobs, long long nctas, const CUtensorMap* tmaps,
-                                  cudaStream_t stream);
+                                  const int* begins, int njobs, long long nctas,
+                                  const CUtensorMap* tmaps, cudaStream_t stream);
 cudaError_t launch_backward_engine(int order, bool exact, LaunchShape shape, const EngineLaunch& L,
                                    long long nctas, const CUtensorMap* tmaps, cudaStream_t stream);
 

@@ -1133,7 +1133,7 @@ struct twi_batch {
     // phases: 0 forward without checkpoints, 1 forward with, 2 gradient
     std::vector<Launch> launches[3];
     size_t njobs[3] = {0, 0, 0};
-    size_t off_tmaps = 0, off_jobs[3] = {0, 0, 0}, total = 0;
+    size_t off_tmaps = 0, off_jobs[3] = {0, 0, 0}, off_begins[3] = {0, 0, 0}, total = 0;
     char* ws = nullptr;
     bool built[3] = {false, false, false};
     cudaStream_t capture_stream = nullptr;
@@ -1190,6 +1190,10 @@ struct twi_batch {
         if (jobs.size() != njobs[phase]) return fail(TWI_ERR_STATE, "batch job count mismatch");
         TWI_CUDA(cudaMemcpy(ws + off_jobs[phase], jobs.data(), jobs.size() * sizeof(MultiJob),
                             cudaMemcpyHostToDevice));
+        std::vector<int> begins(jobs.size());
+        for (size_t i = 0; i < jobs.size(); ++i) begins[i] = jobs[i].cta_begin;
+        TWI_CUDA(cudaMemcpy(ws + off_begins[phase], begins.data(), begins.size() * sizeof(int),
+                            cudaMemcpyHostToDevice));
         built[phase] = true;
         return TWI_OK;
     }
@@ -1198,11 +1202,14 @@ struct twi_batch {
         if (phase == 2)
             for (twi_plan* P : plans) TWI_TRY(P->gradient_prologue(st));
         const MultiJob* base = reinterpret_cast<const MultiJob*>(ws + off_jobs[phase]);
+        const int* begins = reinterpret_cast<const int*>(ws + off_begins[phase]);
         const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
         for (const Launch& L : launches[phase]) {
             cudaError_t e = L.mode == kModeBackward
-                ? launch_backward_multi(order, exact, shape_back, base + L.job0, L.njobs, L.nctas, tm, st)
-                : launch_step_multi(order, exact, L.mode, shape, base + L.job0, L.njobs, L.nctas, tm, st);
+                ? launch_backward_multi(order, exact, shape_back, base + L.job0, begins + L.job0, L.njobs,
+                                        L.nctas, tm, st)
+                : launch_step_multi(order, exact, L.mode, shape, base + L.job0, begins + L.job0, L.njobs,
+                                    L.nctas, tm, st);
             if (e != cudaSuccess)
                 return fail(TWI_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
         }
@@ -1274,7 +1281,10 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
     B->off_tmaps = take(B->plans.size() * kMapsPerPlan * sizeof(CUtensorMap));
-    for (int ph = 0; ph < 3; ++ph) B->off_jobs[ph] = take(B->njobs[ph] * sizeof(MultiJob));
+    for (int ph = 0; ph < 3; ++ph) {
+        B->off_jobs[ph] = take(B->njobs[ph] * sizeof(MultiJob));
+        B->off_begins[ph] = take(B->njobs[ph] * sizeof(int));
+    }
     B->total = off;
     *out = B;
     return TWI_OK;

@@ -610,18 +610,15 @@ step_kernel(const __grid_constant__ CUtensorMap tm_u2, const __grid_constant__ C
 }
 
 // Several plans (different grids, shots, time indices) in one launch: CTA
-// ranges of the jobs are contiguous and ascending in jobs[].cta_begin; the
-// main-height tensor maps of plan p are tmaps[6p .. 6p+2].
+// ranges of the jobs are contiguous and ascending; begins[i] is
+// jobs[i].cta_begin in one compact array (the CTA's job is found by a binary
+// search over it); the main-height tensor maps of plan p are
+// tmaps[6p .. 6p+2].
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __global__ void __launch_bounds__(WZ * 32, kMinCtasPerSm(RZ))
-step_kernel_multi(const MultiJob* __restrict__ jobs, const int njobs,
+step_kernel_multi(const MultiJob* __restrict__ jobs, const int* __restrict__ begins, const int njobs,
                   const CUtensorMap* __restrict__ tmaps) {
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi) {   // last job with cta_begin <= blockIdx.x
-        const int mid = (lo + hi + 1) >> 1;
-        if (jobs[mid].cta_begin <= (int)blockIdx.x) lo = mid;
-        else hi = mid - 1;
-    }
+    const int lo = job_of([&](int i) { return begins[i]; }, njobs, (int)blockIdx.x);
     const MultiJob& J = jobs[lo];
     const CUtensorMap* tm = tmaps + kMapsPerPlan * J.plan;
     // Read through a pointer into global memory, the arguments would have to
@@ -693,6 +690,7 @@ struct LaunchReq {
     const CUtensorMap* tv = nullptr;
     const StepArgs* a = nullptr;
     const MultiJob* jobs = nullptr;
+    const int* begins = nullptr;
     int njobs = 0;
     long long nctas = 0;
     const CUtensorMap* tmaps = nullptr;
@@ -768,7 +766,7 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
                     <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(*q.engine, q.tmaps);
             else
                 step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>
-                    <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.njobs, q.tmaps);
+                    <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.begins, q.njobs, q.tmaps);
         }
     } else {
         int nbc = 0;
@@ -964,10 +962,10 @@ cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
 }
 
 cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
-                              const MultiJob* jobs, int njobs, long long nctas,
+                              const MultiJob* jobs, const int* begins, int njobs, long long nctas,
                               const CUtensorMap* tmaps, cudaStream_t stream) {
     LaunchReq q;
-    q.multi = true, q.jobs = jobs, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    q.multi = true, q.jobs = jobs, q.begins = begins, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
     return launch_req(order, exact, mode, shape, q, stream);
 }
 
