@@ -241,7 +241,8 @@ def run_b200(args):
     opts = PlanOptions(exact=not args.fast, accumulate="kahan", ckpt_interval=args.ckpt,
                        shots_per_cta=args.spc, rows_per_warp=args.rz, use_graphs=True,
                        time_block=args.time_block, reconstruct=args.reconstruct,
-                       split_backward=args.split_backward, persistent=args.persistent)
+                       split_backward=args.split_backward, persistent=args.persistent,
+                       chained=not args.unchained)
     fused = args.reconstruct and not args.split_backward
     tuned_ms = None
     if args.autotune:   # outside the timed region
@@ -458,7 +459,9 @@ def run_b200(args):
                        "adjoint_shots_per_cta": plan.layout.adjoint_shots_per_cta,
                        "time_block": plan.layout.time_block,
                        "launches": "one persistent launch per pass" if args.persistent
-                                   else "one launch per time step (CUDA graph)",
+                                   else "one launch per time step (CUDA graph)" + (
+                                       "" if args.unchained else ", chained: each launch starts "
+                                       "while the previous one drains"),
                        "autotuned": bool(args.autotune),
                        "adjoint_wavefield": ("boundary saving, reverse reconstruction, "
                                              + ("rebuild and adjoint launches" if args.split_backward
@@ -651,6 +654,8 @@ def main():
                          "boundary saving with reverse reconstruction")
     ap.add_argument("--persistent", action="store_true",
                     help="one persistent launch per pass instead of one launch per time step")
+    ap.add_argument("--unchained", action="store_true",
+                    help="every launch waits for the previous one in stream order (no chained launches)")
     ap.add_argument("--split-backward", action="store_true",
                     help="boundary saving: rebuild and adjoint as two launches per step instead of "
                          "the fused backward launch")

@@ -163,6 +163,13 @@ typedef struct twi_problem {
                              wait, with bounded waits, for the group's previous
                              step; 0: one launch per time step.  The same bits
                              either way; not with time_block 2 */
+    int unchained;        /* 0: a run of one-step launches of one kind (a pass, or
+                             a checkpoint segment's recompute or adjoint phase) is
+                             chained: each launch may start its CTAs while the one
+                             before it drains, and a CTA waits (bounded) only for
+                             its shot group of the earlier steps; 1: every launch
+                             waits for the previous one in stream order.  The same
+                             bits either way; not with persistent launches */
 } twi_problem;
 
 /* Byte offsets of the caller-visible regions inside the workspace. */

@@ -127,6 +127,23 @@ def test_persistent_plans_run_one_step_per_item():
         _capi.lib().twi_plan_destroy(h)
 
 
+def test_chained_launch_option():
+    st, _ = _create(unchained=2)
+    assert st == _capi.TWI_ERR_INVALID
+    assert "unchained" in _capi.last_error()
+    # chaining needs one counter per shot group: the workspace grows by at most a few hundred bytes
+    sizes = []
+    for kw in (dict(unchained=0), dict(unchained=1), dict(unchained=0, persistent=1)):
+        st, h = _create(**kw)
+        assert st == _capi.TWI_OK, kw
+        lay = _capi.Layout()
+        assert _capi.lib().twi_plan_layout(h, ctypes.byref(lay)) == 0
+        sizes.append(lay.workspace_bytes)
+        _capi.lib().twi_plan_destroy(h)
+    assert 0 < sizes[0] - sizes[1] <= 4096
+    assert sizes[2] != sizes[0]
+
+
 def test_two_rows_per_warp_runs_one_step_per_launch():
     st, h = _create(rows_per_warp=2, time_block=2)
     assert st == _capi.TWI_ERR_INVALID

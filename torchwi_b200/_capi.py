@@ -39,7 +39,8 @@ class Problem(ctypes.Structure):
                 ("use_graphs", ctypes.c_int), ("wavelet_per_shot", ctypes.c_int),
                 ("forward_only", ctypes.c_int), ("exa", ctypes.c_int),
                 ("time_block", ctypes.c_int), ("reconstruct", ctypes.c_int),
-                ("persistent", ctypes.c_int)]
+                ("persistent", ctypes.c_int),
+                ("unchained", ctypes.c_int)]
 
 
 class Layout(ctypes.Structure):

@@ -71,6 +71,12 @@ __device__ __forceinline__ void backward_boundary(const StepArgs& a, int b, int 
     const int s0 = grp * a.spc, s1 = min(s0 + a.spc, a.nshots);
     const int nb = boundary_cells(ORDER, a.dimx, a.dimz);
     const bool plain = a.acc_mode == kAccPlainPerShot;
+    if (a.chain != nullptr) {
+        __shared__ int sh_go;
+        if (threadIdx.x == 0) sh_go = chain_wait(a, grp);
+        __syncthreads();
+        if (!sh_go) return;
+    }
     for (int idx = part * blockDim.x + threadIdx.x; idx < nb; idx += nbc * blockDim.x) {
         int r, c;
         long long db;   // offset to the first cell inwards
@@ -96,6 +102,7 @@ __device__ __forceinline__ void backward_boundary(const StepArgs& a, int b, int 
             }
         }
     }
+    chain_done(a, grp);
 }
 
 // x neighbours of a lane's four columns at distance 1..NE from warp shuffles;
@@ -144,17 +151,19 @@ __device__ __forceinline__ void update4(const float4 (&win)[ORDER + 1], const fl
 template <int ORDER, bool EXACT, int RZ, int WZ>
 __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUtensorMap* tm_p,
                                               const CUtensorMap* tm_vel, const StepArgs& a,
-                                              const int nbc, const int cta) {
+                                              const int nbc, const int cta_in) {
     using S = BackSmem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
 
+    allow_next_launch();
     const int ngroups = (a.nshots + a.spc - 1) / a.spc;
+    const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
+    const int tiles_z = (a.dimz + TZ - 1) / TZ;
+    const int cta = chain_order(a, cta_in, nbc, ngroups, tiles_x * tiles_z);
     if (cta < nbc * ngroups) {
         backward_boundary<ORDER, EXACT>(a, cta, nbc);
         return;
     }
-    const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
-    const int tiles_z = (a.dimz + TZ - 1) / TZ;
     const int m_id = cta - nbc * ngroups;
     const int tile_x = m_id % tiles_x;
     const int tile_z = (m_id / tiles_x) % tiles_z;
@@ -176,6 +185,8 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
     // the group's source cells, wavelet samples and receiver rows, read once
     __shared__ int sh_src_r[kMaxShotsPerCta], sh_src_c[kMaxShotsPerCta], sh_rec_r[kMaxShotsPerCta];
     __shared__ float sh_wamp[kMaxShotsPerCta];
+    __shared__ int sh_done[STAGES];   // warps done with each stage (last_warp_done)
+    if (threadIdx.x < STAGES) sh_done[threadIdx.x] = 0;
     if (threadIdx.x < nloc) {
         const int s = s_begin + threadIdx.x;
         sh_src_r[threadIdx.x] = a.src_rc[2 * s];
@@ -197,16 +208,23 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
+        // a refill may come from any warp: its tensor loads follow the
+        // chain's acquire only through this thread's own proxy fence
+        if (a.chain != nullptr && k >= STAGES) fence_proxy_async_global();
         mbar_arrive_expect_tx(b, S::STAGE_TX);
         tma_load_3d(st, tm_c, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
         tma_load_3d(st + S::C_FLOATS, tm_p, x0, z0, a.prev_base + s * a.prev_stride, b);
         tma_load_3d(st + S::FIELD_FLOATS, tm_c, x0 - kHaloX, z0 - HZ, a.lcur_base + s * a.lcur_stride, b);
         tma_load_3d(st + S::FIELD_FLOATS + S::C_FLOATS, tm_p, x0, z0, a.lprev_base + s * a.lprev_stride, b);
     };
+    // the velocity tile is static; the fields wait for the chain, if any
+    bool go = true;
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
         tma_load_2d(vs, tm_vel, x0, z0, &bar[0]);
-        for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+        go = chain_wait(a, grp);
+        if (go)
+            for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
     }
 
     const int rl0 = warp * RZ;           // first tile-local row of this warp
@@ -223,10 +241,10 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
 
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
-        if (__syncthreads_or(!ok)) {
+        if (__syncthreads_or(!ok || !go)) {
             if (threadIdx.x == 0) {
-                atomicOr(a.err, 1);
-                drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
+                if (!ok) atomicOr(a.err, 1);
+                if (go) drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
             }
             return;
         }
@@ -268,15 +286,14 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
         const int src_r = sh_src_r[k], src_c = sh_src_c[k], rec_r = sh_rec_r[k];
         const float wamp = sh_wamp[k];
 
-        {
-            const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
-            if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) {
-                    atomicOr(a.err, 1);
-                    drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
-                }
-                return;
+        if (!warp_wait_stage(&bar[1 + (k % STAGES)], (k / STAGES) & 1)) {
+            // the copies never landed: flag it, wait (bounded) for the copies
+            // this warp may have issued, and leave
+            if (lane == 0) {
+                atomicOr(a.err, 1);
+                drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
             }
+            return;
         }
 
         float4 wu[2 * NE + 1], wl[2 * NE + 1];
@@ -390,8 +407,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
             for (int j = 0; j < 2 * NE; ++j) wu[j] = wu[j + 1], wl[j] = wl[j + 1];
         }
 
-        __syncthreads();   // every warp is done with this stage
-        if (threadIdx.x == 0 && k + STAGES < nloc) issue(k + STAGES);
+        if (last_warp_done(sh_done, k, STAGES, WZ) && k + STAGES < nloc) issue(k + STAGES);
     }
 
     if (kahan) {
@@ -405,6 +421,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
             }
         }
     }
+    chain_done(a, grp);
 }
 
 template <int ORDER, bool EXACT, int RZ, int WZ>
@@ -534,6 +551,8 @@ cudaError_t back_one(const BackReq& q, cudaStream_t st) {
     int nbc = 0;
     const int n = back_ctas_of<ORDER, RZ, 4>(*a, &nbc);
     if (n <= 0) return cudaErrorInvalidConfiguration;
+    if (a->chain != nullptr && a->chain_k > 0)
+        return launch_chained(backward_kernel<ORDER, EXACT, RZ, 4>, n, 128, S::BYTES, st, *tc, *tp, *tv, *a, nbc);
     backward_kernel<ORDER, EXACT, RZ, 4><<<dim3((unsigned)n), 128, S::BYTES, st>>>(*tc, *tp, *tv, *a, nbc);
     return cudaGetLastError();
 }

@@ -89,6 +89,14 @@ struct StepArgs {
     int lprev_base, lprev_stride;
     int lcur_base, lcur_stride;
     int lnext_base, lnext_stride;
+    // Chained launches (one launch per step, each free to start its CTAs
+    // while the previous one drains): chain[g] counts the finished CTAs of
+    // shot group g over the chain's launches.  A CTA of group g of the
+    // chain's launch k waits until chain[g] >= k * chain_per_group and adds
+    // one when it is done; chained launches order their CTAs group by group.
+    // Null: stream order alone.
+    unsigned* chain;
+    int chain_k, chain_per_group;
 };
 
 // A persistent launch (twi_persist.cuh): `nsteps` consecutive time steps of

@@ -26,6 +26,7 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 
 #include "twi_kernels.h"
 #include "twi_ptx.cuh"
@@ -67,6 +68,65 @@ __device__ __forceinline__ bool wait_count(const unsigned* count, unsigned targe
         __nanosleep(ns);
         ns = ns < 1024 ? 2 * ns : 1024;
     }
+}
+
+// ---- chained launches (StepArgs::chain) ----------------------------------
+// The stream's next launch, when it allows it, may start its CTAs once every
+// CTA of this launch has started; from then on it takes the SM slots this
+// one gives back.  Its CTAs hold none that this launch still needs, so both
+// make progress; the counters below order the data.
+__device__ __forceinline__ void allow_next_launch() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Body CTA index of launch CTA `cta` when the launch is chained: CTAs run
+// group by group (group g's boundary CTAs, then its interior tiles), so
+// the first CTAs of the next launch wait on the first groups of this one.
+// The body's own order has every group's boundary CTAs first.
+__device__ __forceinline__ int chain_order(const StepArgs& a, int cta, int nbc, int ngroups, int tiles) {
+    if (a.chain == nullptr) return cta;
+    const int per = nbc + tiles;
+    const int g = cta / per, j = cta - g * per;
+    return j < nbc ? g * nbc + j : nbc * ngroups + g * tiles + (j - nbc);
+}
+
+// Thread 0: wait until the chain's earlier launches are done with shot group
+// `grp`, then order the tensor loads after their stores.  False when the
+// wait ran out or another CTA raised the error word.
+__device__ __forceinline__ bool chain_wait(const StepArgs& a, int grp) {
+    if (a.chain == nullptr || a.chain_k <= 0) return true;
+    const bool ok = wait_count(a.chain + grp, (unsigned)a.chain_k * (unsigned)a.chain_per_group, a.err);
+    fence_proxy_async_global();
+    return ok;
+}
+
+// Every thread, after the CTA's last store: release the stores and count the
+// CTA as done for group `grp`.
+__device__ __forceinline__ void chain_done(const StepArgs& a, int grp) {
+    if (a.chain == nullptr) return;
+    fence_proxy_async_global();
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(a.chain + grp, 1u);
+}
+
+// Host: a launch of a chain after its first: it may start while the
+// stream's previous launch is still running (programmatic stream
+// serialization; the kernel's counters order the data).
+template <typename Kernel, typename... Args>
+cudaError_t launch_chained(Kernel kernel, int grid, int threads, size_t smem, cudaStream_t stream,
+                           Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // The persistent work loop.  `body(args, cta)` runs one CTA of a step as a

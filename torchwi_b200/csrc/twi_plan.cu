@@ -193,6 +193,9 @@ struct twi_plan {
     enum { kTabForward = 0, kTabForwardSave = 1, kTabForwardResid = 2, kTabGradient = 3, kTables = 4 };
     size_t off_tab[kTables] = {}, tab_cap[kTables] = {}, off_cnt = 0;
     std::vector<StepArgs> tab_host[kTables];
+    // chained launches (StepArgs::chain): one counter per shot group
+    bool chained = false;
+    size_t off_chain = 0;
     char* ws = nullptr;
     int device = -1;
     CUtensorMap tm_u2{}, tm_u1{}, tm_vel{};
@@ -498,6 +501,44 @@ struct twi_plan {
         return TWI_OK;
     }
 
+    // A step list as launches.  Runs of two or more one-step launches of one
+    // mode are chained when the plan chains: the group counters are zeroed,
+    // then every launch after the run's first may start while the one before
+    // it drains, each CTA waiting for its shot group of the earlier steps.
+    int launch_list(const std::vector<Step>& steps, cudaStream_t st) const {
+        for (size_t i = 0; i < steps.size();) {
+            size_t j = i + 1;
+            while (j < steps.size() && steps[i].nsteps == 1 && steps[j].nsteps == 1 &&
+                   steps[j].mode == steps[i].mode && steps[j].a.spc == steps[i].a.spc)
+                ++j;
+            if (!chained || j - i < 2) {
+                for (size_t t = i; t < j; ++t) TWI_TRY(launch(steps[t].mode, steps[t].a, st, steps[t].nsteps));
+                i = j;
+                continue;
+            }
+            const StepMode mode = steps[i].mode;
+            const bool adj = mode == kModeAdjoint || mode == kModeBackward;
+            const LaunchShape sh = default_shape(adj ? rz_adj : rz);
+            int nbc = 0;
+            const int total = mode == kModeBackward ? backward_ctas(p.order, sh.rows_per_warp, steps[i].a, &nbc)
+                                                    : step_ctas(p.order, sh, steps[i].a, &nbc);
+            const int ngroups = (steps[i].a.nshots + steps[i].a.spc - 1) / steps[i].a.spc;
+            if (total <= 0 || ngroups < 1 || ngroups > p.nshots || total % ngroups != 0)
+                return fail(TWI_ERR_INVALID, "chained launch too large");
+            unsigned* cnt = reinterpret_cast<unsigned*>(ws + off_chain);
+            TWI_CUDA(cudaMemsetAsync(cnt, 0, (size_t)ngroups * sizeof(unsigned), st));
+            for (size_t t = i; t < j; ++t) {
+                StepArgs a = steps[t].a;
+                a.chain = cnt;
+                a.chain_k = (int)(t - i);
+                a.chain_per_group = total / ngroups;
+                TWI_TRY(launch(mode, a, st));
+            }
+            i = j;
+        }
+        return TWI_OK;
+    }
+
     // The steps of table k, one persistent launch per run of the same mode.
     int launch_table(int k, const std::vector<Step>& steps, cudaStream_t st) const {
         const StepArgs* dev = reinterpret_cast<const StepArgs*>(ws + off_tab[k]);
@@ -528,7 +569,7 @@ struct twi_plan {
         if (persist) {
             TWI_TRY(launch_table(forward_table(save, obs), steps, st));
         } else {
-            for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
+            TWI_TRY(launch_list(steps, st));
         }
         if (misfit) {
             cudaError_t e = launch_misfit(F(off_frd), (long long)p.nshots * p.nt * p.nx,
@@ -545,7 +586,7 @@ struct twi_plan {
         if (persist) {
             TWI_TRY(launch_table(kTabGradient, steps, st));
         } else {
-            for (const Step& s : steps) TWI_TRY(launch(s.mode, s.a, st, s.nsteps));
+            TWI_TRY(launch_list(steps, st));
         }
         return gradient_epilogue(st);
     }
@@ -655,6 +696,11 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
                                      "(time_block 2 is not available with them)");
     }
     P->persist = p.persistent == 1;
+    if (p.unchained < 0 || p.unchained > 1) {
+        delete P;
+        return fail(TWI_ERR_INVALID, "unchained must be 0 or 1");
+    }
+    P->chained = !P->persist && p.unchained == 0;
     P->rot = P->tb == 2 ? 4 : 3;
     if (P->recon) {   // no checkpoints: one segment, one virtual-source slot per shot
         P->K = p.nt;
@@ -696,6 +742,7 @@ int twi_plan_create(const twi_problem* prob, twi_plan** out) {
         }
         P->off_cnt = take((size_t)(1 + p.nshots) * sizeof(unsigned));
     }
+    P->off_chain = take(P->chained ? (size_t)p.nshots * sizeof(unsigned) : 0);
     P->total = off;
     *out = P;
     return TWI_OK;

@@ -61,6 +61,12 @@ template <int ORDER, bool EXACT, int MODE>
 __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& d, int b, int nbc) {
     constexpr int NE = ORDER / 2;
     const int grp = b / nbc, part = b - grp * nbc;
+    if (a.chain != nullptr) {
+        __shared__ int sh_go;
+        if (threadIdx.x == 0) sh_go = chain_wait(a, grp);
+        __syncthreads();
+        if (!sh_go) return;
+    }
     const int s0 = grp * a.spc, s1 = min(s0 + a.spc, a.nshots);
     const int nb = boundary_cells(ORDER, a.dimx, a.dimz);
     for (int idx = part * blockDim.x + threadIdx.x; idx < nb; idx += nbc * blockDim.x) {
@@ -125,6 +131,7 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
             }
         }
     }
+    chain_done(a, grp);
 }
 
 // One CTA of one job (a time step of one plan): `cta` indexes the job's CTAs,
@@ -134,17 +141,19 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
 __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUtensorMap* tm_u1p,
                                           const CUtensorMap* tm_velp, const StepArgs& a,
-                                          const StepDyn& d, const int nbc, const int cta) {
+                                          const StepDyn& d, const int nbc, const int cta_in) {
     using S = Smem<ORDER, RZ, WZ>;
     constexpr int NE = S::NE, HZ = S::HZ, TZ = S::TZ, STAGES = S::STAGES;
 
+    allow_next_launch();
     const int ngroups = (a.nshots + a.spc - 1) / a.spc;
+    const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
+    const int tiles_z = (a.dimz + TZ - 1) / TZ;
+    const int cta = chain_order(a, cta_in, nbc, ngroups, tiles_x * tiles_z);
     if (cta < nbc * ngroups) {
         boundary_part<ORDER, EXACT, MODE>(a, d, cta, nbc);
         return;
     }
-    const int tiles_x = (a.dimx + kTileX - 1) / kTileX;
-    const int tiles_z = (a.dimz + TZ - 1) / TZ;
     const int m_id = cta - nbc * ngroups;
     const int tile_x = m_id % tiles_x;
     const int tile_z = (m_id / tiles_x) % tiles_z;
@@ -166,6 +175,8 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     // the group's source cells, wavelet samples and receiver rows, read once
     __shared__ int sh_src_r[kMaxShotsPerCta], sh_src_c[kMaxShotsPerCta], sh_rec_r[kMaxShotsPerCta];
     __shared__ float sh_wamp[kMaxShotsPerCta];
+    __shared__ int sh_done[STAGES];   // warps done with each stage (last_warp_done)
+    if (threadIdx.x < STAGES) sh_done[threadIdx.x] = 0;
     if (threadIdx.x < nloc) {
         const int s = s_begin + threadIdx.x;
         sh_src_r[threadIdx.x] = MODE != kModeAdjoint ? a.src_rc[2 * s] : -1;
@@ -187,14 +198,21 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
+        // a refill may come from any warp: its tensor loads follow the
+        // chain's acquire only through this thread's own proxy fence
+        if (a.chain != nullptr && k >= STAGES) fence_proxy_async_global();
         mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
         tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, d.cur_base + s * d.cur_stride, b);
         tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, d.prev_base + s * d.prev_stride, b);
     };
+    // the velocity tile is static; the fields wait for the chain, if any
+    bool go = true;
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
         tma_load_2d(vs, tm_velp, x0, z0, &bar[0]);
-        for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+        go = chain_wait(a, grp);
+        if (go)
+            for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
     }
 
     const int rl0 = warp * RZ;           // first tile-local row of this warp
@@ -225,10 +243,10 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
 
     {
         const bool ok = mbar_wait_bounded(&bar[0], 0);
-        if (__syncthreads_or(!ok)) {
+        if (__syncthreads_or(!ok || !go)) {
             if (threadIdx.x == 0) {
-                atomicOr(a.err, 1);
-                drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
+                if (!ok) atomicOr(a.err, 1);
+                if (go) drain_stages(&bar[1], STAGES, 0, min(STAGES, nloc));
             }
             return;
         }
@@ -317,15 +335,14 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             }
         }
 
-        {
-            const bool ok = mbar_wait_bounded(&bar[1 + (k % STAGES)], (k / STAGES) & 1);
-            if (__syncthreads_or(!ok)) {
-                if (threadIdx.x == 0) {
-                    atomicOr(a.err, 1);
-                    drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
-                }
-                return;
+        if (!warp_wait_stage(&bar[1 + (k % STAGES)], (k / STAGES) & 1)) {
+            // the copies never landed: flag it, wait (bounded) for the copies
+            // this warp may have issued, and leave
+            if (lane == 0) {
+                atomicOr(a.err, 1);
+                drain_stages(&bar[1], STAGES, k, min(nloc, k + STAGES));
             }
+            return;
         }
 
         float4 win[2 * NE + 1];
@@ -580,8 +597,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
         }
 
-        __syncthreads();   // every warp is done with this stage
-        if (threadIdx.x == 0 && k + STAGES < nloc) issue(k + STAGES);
+        if (last_warp_done(sh_done, k, STAGES, WZ) && k + STAGES < nloc) issue(k + STAGES);
     }
 
     if constexpr (MODE == kModeAdjoint) {
@@ -598,6 +614,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             }
         }
     }
+    chain_done(a, grp);
 }
 
 template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
@@ -772,6 +789,9 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
         int nbc = 0;
         const int n = ctas_of<ORDER, RZ, WZ>(*q.a, &nbc);
         if (n <= 0) return cudaErrorInvalidConfiguration;
+        if (q.a->chain != nullptr && q.a->chain_k > 0)
+            return launch_chained(step_kernel<ORDER, EXACT, MODE, RZ, WZ>, n, WZ * 32, S::BYTES, stream,
+                                  *q.t2, *q.t1, *q.tv, *q.a, nbc);
         step_kernel<ORDER, EXACT, MODE, RZ, WZ>
             <<<dim3((unsigned)n), WZ * 32, S::BYTES, stream>>>(*q.t2, *q.t1, *q.tv, *q.a, nbc);
     }

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "twi_kernels.h"
+#include "twi_ptx.cuh"
 
 namespace twi {
 
@@ -74,6 +75,29 @@ __device__ __forceinline__ int job_of(Begin begin, int njobs, int cta) {
         else hi = mid - 1;
     }
     return lo;
+}
+
+// Shot stages consumed warp by warp.  Every warp waits for a stage's copies
+// itself (all lanes, so each sees the data; the answer is warp-uniform), and
+// the last of the CTA's `nwarps` warps to finish shot k with stage k % stages
+// refills it.  `done[stage]` counts the warps' finishes over the CTA's shots
+// and is never reset, so the last finisher of shot k reads
+// (k / stages + 1) * nwarps - 1; no warp waits for another between shots.
+__device__ __forceinline__ bool warp_wait_stage(uint64_t* bar, uint32_t parity) {
+    return __all_sync(0xffffffffu, mbar_wait_bounded(bar, parity));
+}
+// True on lane 0 of the last warp done with shot k's stage: that lane issues
+// the stage's next copies.  The fences order every lane's reads of the stage
+// before the count, and the count before the refill.
+__device__ __forceinline__ bool last_warp_done(int* done, int k, int stages, int nwarps) {
+    __syncwarp();
+    bool last = false;
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence_block();
+        last = atomicAdd(&done[k % stages], 1) == (k / stages + 1) * nwarps - 1;
+        if (last) __threadfence_block();
+    }
+    return last;
 }
 
 }  // namespace twi

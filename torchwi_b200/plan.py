@@ -53,6 +53,9 @@ class PlanOptions:
     persistent:  run each pass (each checkpoint segment's recompute and
                  adjoint phase) as ONE persistent launch instead of one
                  launch per time step (the same bits).
+    chained:     let each one-step launch of a pass start while the previous
+                 one drains, its CTAs waiting only for their shot group of
+                 the previous step (the same bits; False: plain stream order).
     """
 
     exact: bool = True
@@ -67,6 +70,7 @@ class PlanOptions:
     reconstruct: bool = False
     split_backward: bool = False
     persistent: bool = False
+    chained: bool = True
 
 
 def _stream_handle() -> ctypes.c_void_p:
@@ -98,7 +102,7 @@ def autotune(nx, nz, nshots, order=4, h=10.0, dt=1e-3, options: PlanOptions | No
     dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
     key = (dev.index, nx, nz, nshots, order, o.exact, o.accumulate, o.forward_only, o.exa,
            o.shots_per_cta, o.rows_per_warp, o.time_block, o.reconstruct, o.split_backward,
-           o.persistent)
+           o.persistent, o.chained)
     if key in _TUNED:
         return _TUNED[key]
     import dataclasses
@@ -145,7 +149,7 @@ def _problem(nx, nz, nt, h, dt, nshots, order, wavelet_per_shot, o: PlanOptions)
                    forward_only=int(bool(o.forward_only)), exa=int(bool(o.exa)),
                    time_block=int(o.time_block),
                    reconstruct=(2 if o.split_backward else 1) if o.reconstruct else 0,
-                   persistent=int(bool(o.persistent)))
+                   persistent=int(bool(o.persistent)), unchained=int(not o.chained))
 
 
 class ShotPlan:
