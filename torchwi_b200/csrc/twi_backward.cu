@@ -232,8 +232,6 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
     const int cs = kHaloX + 4 * lane;    // its column in a haloed row
     const bool col_ok = c < a.dimx;
     const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
-    // every lane of the tile on interior columns (CTA-uniform)
-    const bool tile_interior = x0 >= NE && x0 + kTileX <= a.dimx - NE;
     bool cell_in[4];                     // per-cell interior column mask
 #pragma unroll
     for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
@@ -314,9 +312,9 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
             wu[2 * NE] = ld4(uc_s + (rl + HZ + NE) * kBoxX + cs);
             wl[2 * NE] = ld4(lc_s + (rl + HZ + NE) * kBoxX + cs);
             const long long roff = (long long)r * a.pitch + c;
-            // One interior row.  FAST: a row of interior cells only (interior
-            // tile, not a pad row, neither the source nor the receiver row),
-            // so no per-cell or per-row special case is tested.
+            // One interior row.  FAST: neither the source nor the receiver
+            // row, so no per-row special case is tested; in the edge tiles the
+            // lanes holding pad columns mask their stores.
             auto interior_row = [&](auto fast_tag) {
                 constexpr bool FAST = decltype(fast_tag)::value;
                 // ---- u^{it-1}: the forward update run backwards
@@ -360,7 +358,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
                 }
 
                 // pad columns belong to the boundary CTAs: store interior cells only
-                if (FAST || cols_interior) {
+                if (cols_interior) {
                     *reinterpret_cast<float4*>(un_slot + roff) = make_float4(uo[0], uo[1], uo[2], uo[3]);
                     *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(lo[0], lo[1], lo[2], lo[3]);
                 } else {
@@ -371,21 +369,21 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
 
                 // ---- gradient: -virt * lambda with the virtual source of step it
                 if (kahan) {
+                    // every column: the pairs of pad cells and of columns
+                    // past the grid are never read (callers crop the pads)
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        if (FAST || cell_in[m]) {
-                            const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
-                            float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
-                            kahan_add(sm, cm, grad_term<EXACT>(vt, lo[m]));
-                            set_comp(gsum[rr], m, sm);
-                            set_comp(gcmp[rr], m, cm);
-                        }
+                        const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
+                        float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                        kahan_add(sm, cm, grad_term<EXACT>(vt, lo[m]));
+                        set_comp(gsum[rr], m, sm);
+                        set_comp(gcmp[rr], m, cm);
                     }
                 } else {
                     float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + roff;
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        if (FAST || cell_in[m]) {
+                        if (cell_in[m]) {
                             const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
                             g[m] = __fadd_rn(g[m], grad_term<EXACT>(vt, lo[m]));
                         }
@@ -398,7 +396,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
                     *reinterpret_cast<float4*>(un_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
                     *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-            } else if (tile_interior && r != src_r && r != rec_r) {
+            } else if (r != src_r && r != rec_r) {
                 interior_row(std::true_type{});
             } else {
                 interior_row(std::false_type{});

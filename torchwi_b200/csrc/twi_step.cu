@@ -221,8 +221,6 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
     const bool col_ok = c < a.dimx;
     // the lane's four columns are all interior (stencil) columns
     const bool cols_interior = c >= NE && c + 3 < a.dimx - NE;
-    // every lane of the tile on interior columns (CTA-uniform)
-    const bool tile_interior = x0 >= NE && x0 + kTileX <= a.dimx - NE;
     bool cell_in[4];                     // per-cell interior column mask
 #pragma unroll
     for (int m = 0; m < 4; ++m) cell_in[m] = c + m >= NE && c + m < a.dimx - NE;
@@ -414,9 +412,9 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     }
                 }
             } else {
-                // One interior row.  FAST: interior tile, neither the source
-                // nor the receiver row, so no per-cell or per-row special case
-                // is tested.
+                // One interior row.  FAST: neither the source nor the receiver
+                // row, so no per-row special case is tested; in the edge tiles
+                // the lanes holding pad columns mask their stores.
                 auto interior_row = [&](auto fast_tag) {
                     constexpr bool FAST = decltype(fast_tag)::value;
                     float out[4];
@@ -472,7 +470,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                     }
 
                     // pad columns belong to the boundary CTAs: store interior cells only
-                    if (FAST || cols_interior) {
+                    if (cols_interior) {
                         *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
                     } else {
 #pragma unroll
@@ -511,7 +509,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         float* p = a.virt_out +
                                    (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
                                    (long long)r * a.virt_pitch + c;
-                        if ((FAST || cols_interior) && a.virt_vec4) {
+                        if (cols_interior && a.virt_vec4) {
                             *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
                         } else {
 #pragma unroll
@@ -527,7 +525,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         bool changed = false;
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
-                            if (!FAST && !cell_in[m]) continue;
+                            if (!cell_in[m]) continue;
                             const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
                             if (fabsf(vt) > fabsf(comp(ev, m))) {
                                 set_comp(ev, m, vt);
@@ -539,7 +537,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                             }
                         }
                         if (changed) {
-                            if (FAST || cols_interior) {
+                            if (cols_interior) {
                                 *reinterpret_cast<float4*>(a.exa + e0) = ev;
                                 *reinterpret_cast<short4*>(a.iexa + e0) = iv;
                             } else {   // pad columns belong to the boundary CTAs
@@ -560,21 +558,21 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                                        (long long)r * a.pitch + c;
 #pragma unroll
                             for (int m = 0; m < 4; ++m)
-                                if ((FAST || cell_in[m]) && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
+                                if (cell_in[m] && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
                         } else if (a.acc_mode == kAccKahanPerGroup) {
+                            // every column: the pairs of pad cells and of columns
+                            // past the grid are never read (callers crop the pads)
 #pragma unroll
                             for (int m = 0; m < 4; ++m) {
-                                if (FAST || cell_in[m]) {
-                                    float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
-                                    kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
-                                    set_comp(gsum[rr], m, sm);
-                                    set_comp(gcmp[rr], m, cm);
-                                }
+                                float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                                kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                set_comp(gsum[rr], m, sm);
+                                set_comp(gcmp[rr], m, cm);
                             }
                         } else if (a.acc_mode == kAccPlainPerShot) {
                             float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
                                        (long long)r * a.pitch + c;
-                            if (FAST || cols_interior) {
+                            if (cols_interior) {
                                 float4 gv = ld4(g);
 #pragma unroll
                                 for (int m = 0; m < 4; ++m)
@@ -590,7 +588,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
                         }
                     }
                 };
-                if (tile_interior && r != src_r && r != rec_r) interior_row(std::true_type{});
+                if (r != src_r && r != rec_r) interior_row(std::true_type{});
                 else interior_row(std::false_type{});
             }
 #pragma unroll
