@@ -514,7 +514,8 @@ def run_config4(args):
     models = synthetic.config4()
     if args.models:
         models = models[:args.models]
-    opts = PlanOptions(exact=not args.fast, accumulate="kahan", reconstruct=not args.checkpoints)
+    opts = PlanOptions(exact=not args.fast, accumulate="kahan", reconstruct=not args.checkpoints,
+                       chained=not args.unchained)
     free, _ = torch.cuda.mem_get_info(dev)
     budget = int(free * 0.80)
     fps = [footprint_bytes(m.nx, m.nz, m.nt, m.nshots, 4, options=opts) for m in models]
@@ -575,6 +576,8 @@ def run_config4(args):
         torch.cuda.empty_cache()
     print(json.dumps({"workload": "config4 uneven batch", "metric": "shot-gradients/s",
                       "adjoint_wavefield": "checkpoints" if args.checkpoints else "boundary saving, fused backward",
+                      "launches": "stream order" if args.unchained
+                                  else "chained where one launch is at most 8 waves of CTAs",
                       "value": shots / (total_ms / 1e3), "unit": "shot-gradients/s",
                       "gcell_per_s": cells / (total_ms / 1e3) / 1e9, "models": len(models),
                       "shots": shots, "ms_total": total_ms, "waves": per_wave,

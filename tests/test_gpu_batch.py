@@ -23,23 +23,29 @@ def _plan(s, opts):
     return p
 
 
-@pytest.mark.parametrize("accumulate,graphs,rz,recon", [("plain", True, 0, False), ("plain", False, 0, False),
-                                                        ("kahan", True, 0, False), ("kahan", False, 0, False),
-                                                        ("kahan", True, 2, False), ("plain", True, 0, True),
-                                                        ("kahan", True, 0, True), ("kahan", False, 4, True)])
-def test_batch_equals_plans_alone(accumulate, graphs, rz, recon):
+@pytest.mark.parametrize("accumulate,graphs,rz,recon,chained",
+                         [("plain", True, 0, False, True), ("plain", False, 0, False, True),
+                          ("kahan", True, 0, False, True), ("kahan", False, 0, False, True),
+                          ("kahan", True, 2, False, True), ("plain", True, 0, True, True),
+                          ("kahan", True, 0, True, True), ("kahan", False, 4, True, True),
+                          ("kahan", True, 0, True, False), ("plain", True, 0, False, False)])
+def test_batch_equals_plans_alone(accumulate, graphs, rz, recon, chained):
     """recon: boundary-saving plans, whose backward steps are fused launches
-    (one multi-plan launch of the fused backward kernel per step)."""
+    (one multi-plan launch of the fused backward kernel per step).  chained:
+    runs of like launches start while the previous one drains (the default);
+    the plans alone run in stream order either way."""
     surveys = [synthetic.small_case(order=4, **c) for c in CASES]
     opts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs, rows_per_warp=rz,
-                       reconstruct=recon)
+                       reconstruct=recon, chained=False)
+    bopts = PlanOptions(accumulate=accumulate, ckpt_interval=11, use_graphs=graphs, rows_per_warp=rz,
+                        reconstruct=recon, chained=chained)
     alone = []
     for s in surveys:
         p = _plan(s, opts)
         frd = p.forward(save_checkpoints=True).clone()
         g = p.gradient(0.25 * frd).clone()
         alone.append((frd.cpu().numpy(), g.cpu().numpy()))
-    plans = [_plan(s, opts) for s in surveys]
+    plans = [_plan(s, bopts) for s in surveys]
     batch = PlanBatch(plans)
     for rep in range(2):   # a second call replays the captured graphs
         gathers = [g.clone() for g in batch.forward(save_checkpoints=True)]

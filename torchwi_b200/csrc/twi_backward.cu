@@ -208,9 +208,6 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
-        // a refill may come from any warp: its tensor loads follow the
-        // chain's acquire only through this thread's own proxy fence
-        if (a.chain != nullptr && k >= STAGES) fence_proxy_async_global();
         mbar_arrive_expect_tx(b, S::STAGE_TX);
         tma_load_3d(st, tm_c, x0 - kHaloX, z0 - HZ, a.cur_base + s * a.cur_stride, b);
         tma_load_3d(st + S::C_FLOATS, tm_p, x0, z0, a.prev_base + s * a.prev_stride, b);
@@ -247,6 +244,9 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
             return;
         }
     }
+    // any warp may refill a stage later: every thread orders its tensor
+    // loads after the chain's acquire (thread 0's, through the barrier above)
+    if (a.chain != nullptr && a.chain_k > 0) fence_proxy_async_global();
     // per-cell constants over all shots: v*v*dt^2/h^2 and the virtual-source
     // coefficient (columns past the grid hold v = 0: kept finite, never stored)
     float4 vvreg[RZ], qreg[RZ];
@@ -500,6 +500,8 @@ struct BackReq {
     long long nctas = 0;
     const CUtensorMap* tmaps = nullptr;
     const EngineLaunch* engine = nullptr;
+    bool chained = false;   // jobs: a later launch of a chain
+    int* occupancy = nullptr;   // set: CTAs per SM of the one-plan kernel, nothing launched
 };
 
 template <int ORDER, bool EXACT, int RZ>
@@ -527,11 +529,17 @@ cudaError_t back_one(const BackReq& q, cudaStream_t st) {
         if (e != cudaSuccess) return e;
         configured.fetch_or(1ull << dev, std::memory_order_relaxed);
     }
+    if (q.occupancy)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(q.occupancy, backward_kernel<ORDER, EXACT, RZ, 4>, 128,
+                                                             S::BYTES);
     if (q.jobs || q.engine) {
         if (q.nctas <= 0 || q.nctas > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
         if (q.engine)
             backward_kernel_engine<ORDER, EXACT, RZ, 4>
                 <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(*q.engine, q.tmaps);
+        else if (q.chained)
+            return launch_chained(backward_kernel_multi<ORDER, EXACT, RZ, 4>, (int)q.nctas, 128, S::BYTES, st,
+                                  q.jobs, q.begins, q.njobs, q.tmaps);
         else
             backward_kernel_multi<ORDER, EXACT, RZ, 4>
                 <<<dim3((unsigned)q.nctas), 128, S::BYTES, st>>>(q.jobs, q.begins, q.njobs, q.tmaps);
@@ -603,10 +611,11 @@ cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape,
 
 cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
                                   const int* begins, int njobs, long long nctas,
-                                  const CUtensorMap* tmaps, cudaStream_t stream) {
+                                  const CUtensorMap* tmaps, cudaStream_t stream, bool chained) {
     if (shape.warps != 4) return cudaErrorInvalidValue;
     BackReq q;
     q.jobs = jobs, q.begins = begins, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    q.chained = chained;
     return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
 }
 
@@ -616,6 +625,14 @@ cudaError_t launch_backward_engine(int order, bool exact, LaunchShape shape, con
     BackReq q;
     q.engine = &L, q.nctas = nctas, q.tmaps = tmaps;
     return back_dispatch(order, exact, shape.rows_per_warp, q, stream);
+}
+
+int backward_resident_ctas(int order, bool exact, LaunchShape shape) {
+    if (shape.warps != 4) return 0;
+    int n = 0;
+    BackReq q;
+    q.occupancy = &n;
+    return back_dispatch(order, exact, shape.rows_per_warp, q, nullptr) == cudaSuccess ? n : 0;
 }
 
 cudaError_t prepare_backward(int order, bool exact, LaunchShape shape) {

@@ -184,11 +184,24 @@ cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
 // CTAs a single-plan launch of `a` uses, and its boundary CTAs per shot group.
 int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc);
 
+// CTAs of the single-plan kernel resident per SM on the current device (0 on
+// error); with the SM count this gives a launch's number of waves.
+int step_resident_ctas(int order, bool exact, StepMode mode, LaunchShape shape);
+int backward_resident_ctas(int order, bool exact, LaunchShape shape);
+
+// Chained launches pay a fixed cost per CTA (the counter poll before its first
+// copies, the release after its last store) and win back about half a wave
+// of tail per launch, so runs are chained only while one launch is at most
+// this many waves of CTAs.
+constexpr double kChainMaxWaves = 8.0;
+
 // One launch covering several jobs (tensor maps in device memory);
-// begins[i] = jobs[i].cta_begin, ascending.
+// begins[i] = jobs[i].cta_begin, ascending.  `chained`: a later launch of a
+// chain (the jobs' arguments carry its counters), free to start while the
+// stream's previous launch drains.
 cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
                               const MultiJob* jobs, const int* begins, int njobs, long long nctas,
-                              const CUtensorMap* tmaps, cudaStream_t stream);
+                              const CUtensorMap* tmaps, cudaStream_t stream, bool chained = false);
 
 // One engine launch (job entries in device memory, index in parameters).
 cudaError_t launch_step_engine(int order, bool exact, StepMode mode, LaunchShape shape,
@@ -252,7 +265,7 @@ cudaError_t launch_backward_persistent(int order, bool exact, LaunchShape shape,
 // tensor maps.
 cudaError_t launch_backward_multi(int order, bool exact, LaunchShape shape, const MultiJob* jobs,
                                   const int* begins, int njobs, long long nctas,
-                                  const CUtensorMap* tmaps, cudaStream_t stream);
+                                  const CUtensorMap* tmaps, cudaStream_t stream, bool chained = false);
 cudaError_t launch_backward_engine(int order, bool exact, LaunchShape shape, const EngineLaunch& L,
                                    long long nctas, const CUtensorMap* tmaps, cudaStream_t stream);
 

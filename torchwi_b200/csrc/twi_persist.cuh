@@ -101,13 +101,16 @@ __device__ __forceinline__ bool chain_wait(const StepArgs& a, int grp) {
 }
 
 // Every thread, after the CTA's last store: release the stores and count the
-// CTA as done for group `grp`.
+// CTA as done for group `grp`.  The CTA barrier orders every thread's stores
+// before thread 0's release add, and a release is cumulative, so the one add
+// releases them all (the form a grid-wide barrier takes) without stalling
+// thread 0 on a fence; the readers order their tensor loads after their
+// acquire with their own proxy fence.
 __device__ __forceinline__ void chain_done(const StepArgs& a, int grp) {
     if (a.chain == nullptr) return;
-    fence_proxy_async_global();
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(a.chain + grp, 1u);
+    if (threadIdx.x == 0)
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(a.chain + grp) : "memory");
 }
 
 // Host: a launch of a chain after its first: it may start while the

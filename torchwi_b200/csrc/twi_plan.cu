@@ -108,6 +108,18 @@ int make_map(CUtensorMap* tm, const void* base, int dimx, int dimz, long long ns
     return TWI_OK;
 }
 
+// Waves of CTAs of a launch of `nctas` CTAs of the one-plan kernel of this
+// mode and shape on the current device (a large number when unknown).
+double launch_waves(int order, bool exact, StepMode mode, LaunchShape sh, long long nctas) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+        return 1e30;
+    const int per_sm = mode == kModeBackward ? backward_resident_ctas(order, exact, sh)
+                                             : step_resident_ctas(order, exact, mode, sh);
+    return per_sm > 0 ? (double)nctas / ((double)per_sm * sms) : 1e30;
+}
+
 // Cell lookup exactly as the reference: FP32 division, truncation toward 0
 // (propagator_cpu.cpp:44-48).
 int cell_of(float coord, float h) { return static_cast<int>(coord / h); }
@@ -501,6 +513,11 @@ struct twi_plan {
         return TWI_OK;
     }
 
+    // Waves of CTAs of one single-plan launch of `nctas` CTAs on this device.
+    double launch_waves(StepMode mode, LaunchShape sh, long long nctas) const {
+        return twi::launch_waves(p.order, p.exact != 0, mode, sh, nctas);
+    }
+
     // A step list as launches.  Runs of two or more one-step launches of one
     // mode are chained when the plan chains: the group counters are zeroed,
     // then every launch after the run's first may start while the one before
@@ -525,6 +542,11 @@ struct twi_plan {
             const int ngroups = (steps[i].a.nshots + steps[i].a.spc - 1) / steps[i].a.spc;
             if (total <= 0 || ngroups < 1 || ngroups > p.nshots || total % ngroups != 0)
                 return fail(TWI_ERR_INVALID, "chained launch too large");
+            if (launch_waves(mode, sh, total) > kChainMaxWaves) {   // the tail is too small to pay for it
+                for (size_t t = i; t < j; ++t) TWI_TRY(launch(steps[t].mode, steps[t].a, st, steps[t].nsteps));
+                i = j;
+                continue;
+            }
             unsigned* cnt = reinterpret_cast<unsigned*>(ws + off_chain);
             TWI_CUDA(cudaMemsetAsync(cnt, 0, (size_t)ngroups * sizeof(unsigned), st));
             for (size_t t = i; t < j; ++t) {
@@ -1176,7 +1198,14 @@ struct twi_batch {
         size_t job0;   // first job in the phase's table
         int njobs;
         long long nctas;
+        bool reset = false;   // first launch of a chain: zero the counters first
+        bool pdl = false;     // later launch of a chain
     };
+    // chained launches (StepArgs::chain) when every plan chains: plan i's
+    // shot groups count in the counters from chain_off[i] on
+    bool chained = true;
+    size_t off_chain = 0, chain_count = 0;
+    std::vector<size_t> chain_off;
     // phases: 0 forward without checkpoints, 1 forward with, 2 gradient
     std::vector<Launch> launches[3];
     size_t njobs[3] = {0, 0, 0};
@@ -1235,6 +1264,7 @@ struct twi_batch {
             }
         }
         if (jobs.size() != njobs[phase]) return fail(TWI_ERR_STATE, "batch job count mismatch");
+        if (chained) chain_launches(launches[phase], jobs);
         TWI_CUDA(cudaMemcpy(ws + off_jobs[phase], jobs.data(), jobs.size() * sizeof(MultiJob),
                             cudaMemcpyHostToDevice));
         std::vector<int> begins(jobs.size());
@@ -1245,6 +1275,42 @@ struct twi_batch {
         return TWI_OK;
     }
 
+    // Runs of two or more consecutive launches of one mode over the same
+    // jobs (same plans, shapes and CTA counts) become chains: their jobs'
+    // arguments carry the plan's counters, the step's place in the chain and
+    // the CTAs per shot group.
+    void chain_launches(std::vector<Launch>& Ls, std::vector<MultiJob>& jobs) const {
+        auto same = [&](const Launch& x, const Launch& y) {
+            if (x.mode != y.mode || x.njobs != y.njobs) return false;
+            for (int j = 0; j < x.njobs; ++j) {
+                const MultiJob& p = jobs[x.job0 + j];
+                const MultiJob& q = jobs[y.job0 + j];
+                if (p.plan != q.plan || p.ncta != q.ncta || p.nbc != q.nbc || p.a.spc != q.a.spc) return false;
+            }
+            return true;
+        };
+        unsigned* cnt = reinterpret_cast<unsigned*>(ws + off_chain);
+        for (size_t i = 0; i < Ls.size();) {
+            size_t j = i + 1;
+            while (j < Ls.size() && same(Ls[i], Ls[j])) ++j;
+            const LaunchShape sh = Ls[i].mode == kModeBackward ? shape_back : shape;
+            if (j - i >= 2 && launch_waves(order, exact, Ls[i].mode, sh, Ls[i].nctas) <= kChainMaxWaves) {
+                for (size_t t = i; t < j; ++t) {
+                    Ls[t].reset = t == i;
+                    Ls[t].pdl = t > i;
+                    for (int q = 0; q < Ls[t].njobs; ++q) {
+                        MultiJob& J = jobs[Ls[t].job0 + q];
+                        const int ng = (J.a.nshots + J.a.spc - 1) / J.a.spc;
+                        J.a.chain = cnt + chain_off[J.plan];
+                        J.a.chain_k = (int)(t - i);
+                        J.a.chain_per_group = J.ncta / ng;
+                    }
+                }
+            }
+            i = j;
+        }
+    }
+
     int enqueue(int phase, cudaStream_t st) const {
         if (phase == 2)
             for (twi_plan* P : plans) TWI_TRY(P->gradient_prologue(st));
@@ -1252,11 +1318,12 @@ struct twi_batch {
         const int* begins = reinterpret_cast<const int*>(ws + off_begins[phase]);
         const CUtensorMap* tm = reinterpret_cast<const CUtensorMap*>(ws + off_tmaps);
         for (const Launch& L : launches[phase]) {
+            if (L.reset) TWI_CUDA(cudaMemsetAsync(ws + off_chain, 0, chain_count * sizeof(unsigned), st));
             cudaError_t e = L.mode == kModeBackward
                 ? launch_backward_multi(order, exact, shape_back, base + L.job0, begins + L.job0, L.njobs,
-                                        L.nctas, tm, st)
+                                        L.nctas, tm, st, L.pdl)
                 : launch_step_multi(order, exact, L.mode, shape, base + L.job0, begins + L.job0, L.njobs,
-                                    L.nctas, tm, st);
+                                    L.nctas, tm, st, L.pdl);
             if (e != cudaSuccess)
                 return fail(TWI_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
         }
@@ -1319,8 +1386,11 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
             return fail(TWI_ERR_INVALID, "plans of a batch must share order, arithmetic and rows_per_warp");
         }
         B->plans.push_back(P);
+        B->chained = B->chained && P->chained;
     }
     for (twi_plan* P : B->plans) {
+        B->chain_off.push_back(B->chain_count);
+        B->chain_count += (size_t)P->p.nshots;   // at least one counter per shot group of any mode
         B->njobs[0] += P->p.nt;
         B->njobs[1] += P->p.nt;
         B->njobs[2] += (P->fused_back ? 1 : 2) * (size_t)P->p.nt;   // fused backward: one job per step
@@ -1332,6 +1402,7 @@ int twi_batch_create(twi_plan* const* plans, int nplans, twi_batch** out) {
         B->off_jobs[ph] = take(B->njobs[ph] * sizeof(MultiJob));
         B->off_begins[ph] = take(B->njobs[ph] * sizeof(int));
     }
+    B->off_chain = take(B->chained ? B->chain_count * sizeof(unsigned) : 0);
     B->total = off;
     *out = B;
     return TWI_OK;

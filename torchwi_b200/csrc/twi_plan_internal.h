@@ -34,6 +34,9 @@ int cell_of(float coord, float h);
 int shot_cells(float sx, float sy, float ry, float h, int nx, int nz, int ne, int dimz, int* src_r,
                int* src_c, int* rec_r);
 void set_last_error(const std::string& msg);
+// Waves of CTAs of a one-plan launch of `nctas` CTAs of this mode and shape
+// on the current device (huge when the device cannot be queried).
+double launch_waves(int order, bool exact, StepMode mode, LaunchShape sh, long long nctas);
 
 }  // namespace twi
 

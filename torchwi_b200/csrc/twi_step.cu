@@ -198,9 +198,6 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
         uint64_t* b = &bar[1 + (k % STAGES)];
-        // a refill may come from any warp: its tensor loads follow the
-        // chain's acquire only through this thread's own proxy fence
-        if (a.chain != nullptr && k >= STAGES) fence_proxy_async_global();
         mbar_arrive_expect_tx(b, S::U2_TX + S::U1_TX);
         tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, d.cur_base + s * d.cur_stride, b);
         tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, d.prev_base + s * d.prev_stride, b);
@@ -249,6 +246,9 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             return;
         }
     }
+    // any warp may refill a stage later: every thread orders its tensor
+    // loads after the chain's acquire (thread 0's, through the barrier above)
+    if (a.chain != nullptr && a.chain_k > 0) fence_proxy_async_global();
     // per-cell constants over all shots: v*v*dt^2/h^2, and for the recompute
     // the virtual-source coefficient; v itself stays in shared memory
     float4 vvreg[RZ];
@@ -712,7 +712,9 @@ struct LaunchReq {
     const EngineLaunch* engine = nullptr;
     const PersistLaunch* persist = nullptr;
     bool multi = false;
+    bool chained = false;   // multi: a later launch of a chain
     bool configure_only = false;
+    int* occupancy = nullptr;   // set: CTAs per SM of the one-plan kernel, nothing launched
 };
 
 template <int ORDER, int RZ, int WZ>
@@ -761,6 +763,9 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
     using S = Smem<ORDER, RZ, WZ>;
     cudaError_t e = configure_one<ORDER, EXACT, MODE, RZ, WZ>();
     if (e != cudaSuccess || q.configure_only) return e;
+    if (q.occupancy)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(q.occupancy, step_kernel<ORDER, EXACT, MODE, RZ, WZ>,
+                                                             WZ * 32, S::BYTES);
     if (q.persist) {
         const long long items = (long long)q.persist->nsteps * q.persist->ngroups * q.persist->per_group;
         int grid = 0;
@@ -779,6 +784,9 @@ cudaError_t launch_one(const LaunchReq& q, cudaStream_t stream) {
             if (q.engine)
                 step_kernel_engine<ORDER, EXACT, MODE, RZ, WZ>
                     <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(*q.engine, q.tmaps);
+            else if (q.chained)
+                return launch_chained(step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>, (int)q.nctas, WZ * 32,
+                                      S::BYTES, stream, q.jobs, q.begins, q.njobs, q.tmaps);
             else
                 step_kernel_multi<ORDER, EXACT, MODE, RZ, WZ>
                     <<<dim3((unsigned)q.nctas), WZ * 32, S::BYTES, stream>>>(q.jobs, q.begins, q.njobs, q.tmaps);
@@ -981,9 +989,10 @@ cudaError_t launch_step(int order, bool exact, StepMode mode, LaunchShape shape,
 
 cudaError_t launch_step_multi(int order, bool exact, StepMode mode, LaunchShape shape,
                               const MultiJob* jobs, const int* begins, int njobs, long long nctas,
-                              const CUtensorMap* tmaps, cudaStream_t stream) {
+                              const CUtensorMap* tmaps, cudaStream_t stream, bool chained) {
     LaunchReq q;
     q.multi = true, q.jobs = jobs, q.begins = begins, q.njobs = njobs, q.nctas = nctas, q.tmaps = tmaps;
+    q.chained = chained;
     return launch_req(order, exact, mode, shape, q, stream);
 }
 
@@ -1002,6 +1011,13 @@ cudaError_t launch_step_engine(int order, bool exact, StepMode mode, LaunchShape
     LaunchReq q;
     q.engine = &L, q.nctas = nctas, q.tmaps = tmaps;
     return launch_req(order, exact, mode, shape, q, stream);
+}
+
+int step_resident_ctas(int order, bool exact, StepMode mode, LaunchShape shape) {
+    int n = 0;
+    LaunchReq q;
+    q.occupancy = &n;
+    return launch_req(order, exact, mode, shape, q, nullptr) == cudaSuccess ? n : 0;
 }
 
 int step_ctas(int order, LaunchShape shape, const StepArgs& a, int* nbc) {
