@@ -246,6 +246,14 @@ int twi_plan_destroy(twi_plan* plan);
  * limit of `limit_us` microseconds and returns TWI_OK when the wait ran out
  * and was reported as designed; *elapsed_ms gets the kernel's duration. */
 int twi_check_wait_timeout(int limit_us, float* elapsed_ms, void* stream);
+/* The same for the counter wait of chained and persistent launches (a CTA
+ * waiting until its shot group of the earlier steps is done): with
+ * preset_error = 0 the counter never reaches its target and the wait must run
+ * out after `limit_us` and raise the error word; with preset_error = 1 the
+ * word already holds another CTA's error and the wait must leave at once.
+ * TWI_OK when the wait ended as designed; *elapsed_ms gets the kernel's
+ * duration. */
+int twi_check_counter_wait(int limit_us, int preset_error, float* elapsed_ms, void* stream);
 /* Workspace bytes a plan of `prob` needs (host only; admission control). */
 int twi_plan_footprint_bytes(const twi_problem* prob, size_t* bytes);
 

@@ -82,6 +82,7 @@ SIGNATURES = {
     "twi_plan_destroy": [_vp],
     "twi_plan_footprint_bytes": [_vp, ctypes.POINTER(ctypes.c_size_t)],
     "twi_check_wait_timeout": [_i, ctypes.POINTER(ctypes.c_float), _vp],
+    "twi_check_counter_wait": [_i, _i, ctypes.POINTER(ctypes.c_float), _vp],
     "twi_autotune_scratch_bytes": [_vp, ctypes.POINTER(ctypes.c_size_t)],
     "twi_autotune": [_vp, _vp, ctypes.c_size_t, _vp, _vp, ctypes.POINTER(ctypes.c_float)],
     "twi_batch_create": [ctypes.POINTER(_vp), _i, ctypes.POINTER(_vp)],

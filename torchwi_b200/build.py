@@ -18,7 +18,8 @@ OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libtwi_b200.so")
 INCLUDE = os.path.join(REPO, "include")
 SOURCES = ["twi_step.cu", "twi_step2.cu", "twi_backward.cu", "twi_plan.cu", "twi_noalloc.cu", "twi_engine.cu", "twi_diag.cu"]
-HEADERS = ["twi_cell.cuh", "twi_kernels.h", "twi_ptx.cuh", "twi_tile.cuh", "twi_plan_internal.h"]
+HEADERS = ["twi_cell.cuh", "twi_kernels.h", "twi_ptx.cuh", "twi_tile.cuh", "twi_persist.cuh",
+           "twi_plan_internal.h"]
 
 NVCC_FLAGS = [
     "-O3", "-lineinfo", "-std=c++17",

@@ -51,23 +51,28 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Thread 0 only: wait until *count >= target.  False when the wait ran out
-// (bit 1 of *err raised) or another CTA reported an error.
-// Polls back off from 32 ns to 1 µs so that CTAs waiting on one counter do
-// not flood its L2 line.
-__device__ __forceinline__ bool wait_count(const unsigned* count, unsigned target, int* err) {
+// Thread 0 only: wait until *count >= target, for at most `limit_ns` of
+// wall time and at most kMaxCountPolls polls (a second bound in case the
+// timer does not advance).  False when the wait ran out (bit 1 of *err
+// raised) or another CTA reported an error.  Polls back off from 32 ns to
+// 1 µs so that CTAs waiting on one counter do not flood its L2 line.
+constexpr uint32_t kMaxCountPolls = 1u << 24;
+__device__ __forceinline__ bool wait_count_for(const unsigned* count, unsigned target, int* err,
+                                               uint64_t limit_ns) {
     const uint64_t t0 = globaltimer_ns();
     unsigned ns = 32;
-    for (uint32_t i = 0;; ++i) {
+    for (uint32_t i = 0; i < kMaxCountPolls; ++i) {
         if (ld_acquire_u32(count) >= target) return true;
         if (ld_volatile_s32(err) != 0) return false;
-        if ((i & 15u) == 15u && globaltimer_ns() - t0 > kWaitLimitNs) {
-            atomicOr(err, 2);
-            return false;
-        }
+        if ((i & 15u) == 15u && globaltimer_ns() - t0 > limit_ns) break;
         __nanosleep(ns);
         ns = ns < 1024 ? 2 * ns : 1024;
     }
+    atomicOr(err, 2);
+    return false;
+}
+__device__ __forceinline__ bool wait_count(const unsigned* count, unsigned target, int* err) {
+    return wait_count_for(count, target, err, kWaitLimitNs);
 }
 
 // ---- chained launches (StepArgs::chain) ----------------------------------
