@@ -194,16 +194,6 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
         sh_rec_r[threadIdx.x] = a.rec_row[s];
         sh_wamp[threadIdx.x] = a.wav[(long long)s * a.wav_stride + a.it];
     }
-    if (threadIdx.x == 0) {
-        prefetch_tmap(tm_c);
-        prefetch_tmap(tm_p);
-        prefetch_tmap(tm_vel);
-#pragma unroll
-        for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-
     auto issue = [&](int k) {
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
@@ -214,14 +204,33 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
         tma_load_3d(st + S::FIELD_FLOATS, tm_c, x0 - kHaloX, z0 - HZ, a.lcur_base + s * a.lcur_stride, b);
         tma_load_3d(st + S::FIELD_FLOATS + S::C_FLOATS, tm_p, x0, z0, a.lprev_base + s * a.lprev_stride, b);
     };
-    // the velocity tile is static; the fields wait for the chain, if any
-    bool go = true;
+    // Thread 0 sets up the stage barriers, issues the static velocity tile
+    // and, when the launch waits for nothing, the first stages; meanwhile
+    // lane 0 of warp 1 waits for the chain, if any, so that a chained
+    // launch's field copies go out right after the CTA barrier.
+    const bool chained_wait = a.chain != nullptr && a.chain_k > 0;
+    __shared__ int sh_chain_ok;
     if (threadIdx.x == 0) {
+        prefetch_tmap(tm_c);
+        prefetch_tmap(tm_p);
+        prefetch_tmap(tm_vel);
+#pragma unroll
+        for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
+        fence_barrier_init();
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
         tma_load_2d(vs, tm_vel, x0, z0, &bar[0]);
-        go = chain_wait(a, grp);
-        if (go)
+        if (!chained_wait)
             for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+    }
+    if (chained_wait && threadIdx.x == 32) sh_chain_ok = chain_wait(a, grp) ? 1 : 0;
+    __syncthreads();
+    bool go = true;
+    if (chained_wait && threadIdx.x == 0) {
+        go = sh_chain_ok != 0;
+        if (go) {
+            fence_proxy_async_global();   // these tensor loads after warp 1's acquire
+            for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+        }
     }
 
     const int rl0 = warp * RZ;           // first tile-local row of this warp

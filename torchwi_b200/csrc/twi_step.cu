@@ -184,16 +184,6 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         sh_wamp[threadIdx.x] = MODE != kModeAdjoint ? a.wav[(long long)s * a.wav_stride + d.it] : 0.f;
         sh_rec_r[threadIdx.x] = a.rec_row[s];
     }
-    if (threadIdx.x == 0) {
-        prefetch_tmap(tm_u2p);
-        prefetch_tmap(tm_u1p);
-        prefetch_tmap(tm_velp);
-#pragma unroll
-        for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-
     auto issue = [&](int k) {
         const int s = s_begin + k;
         float* st = stage0 + (k % STAGES) * S::STAGE_FLOATS;
@@ -202,14 +192,33 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
         tma_load_3d(st, tm_u2p, x0 - kHaloX, z0 - HZ, d.cur_base + s * d.cur_stride, b);
         tma_load_3d(st + S::U2_FLOATS, tm_u1p, x0, z0, d.prev_base + s * d.prev_stride, b);
     };
-    // the velocity tile is static; the fields wait for the chain, if any
-    bool go = true;
+    // Thread 0 sets up the stage barriers, issues the static velocity tile
+    // and, when the launch waits for nothing, the first stages; meanwhile
+    // lane 0 of warp 1 waits for the chain, if any, so that a chained
+    // launch's field copies go out right after the CTA barrier.
+    const bool chained_wait = a.chain != nullptr && a.chain_k > 0;
+    __shared__ int sh_chain_ok;
     if (threadIdx.x == 0) {
+        prefetch_tmap(tm_u2p);
+        prefetch_tmap(tm_u1p);
+        prefetch_tmap(tm_velp);
+#pragma unroll
+        for (int i = 0; i < 1 + STAGES; ++i) mbar_init(&bar[i], 1);
+        fence_barrier_init();
         mbar_arrive_expect_tx(&bar[0], S::V_TX);
         tma_load_2d(vs, tm_velp, x0, z0, &bar[0]);
-        go = chain_wait(a, grp);
-        if (go)
+        if (!chained_wait)
             for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+    }
+    if (chained_wait && threadIdx.x == 32) sh_chain_ok = chain_wait(a, grp) ? 1 : 0;
+    __syncthreads();
+    bool go = true;
+    if (chained_wait && threadIdx.x == 0) {
+        go = sh_chain_ok != 0;
+        if (go) {
+            fence_proxy_async_global();   // these tensor loads after warp 1's acquire
+            for (int k = 0; k < STAGES && k < nloc; ++k) issue(k);
+        }
     }
 
     const int rl0 = warp * RZ;           // first tile-local row of this warp
