@@ -51,7 +51,7 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar) {
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Thread 0 only: wait until *count >= target, for at most `limit_ns` of
+// One thread of the CTA: wait until *count >= target, for at most `limit_ns` of
 // wall time and at most kMaxCountPolls polls (a second bound in case the
 // timer does not advance).  False when the wait ran out (bit 1 of *err
 // raised) or another CTA reported an error.  Polls back off from 32 ns to
@@ -95,9 +95,12 @@ __device__ __forceinline__ int chain_order(const StepArgs& a, int cta, int nbc, 
     return j < nbc ? g * nbc + j : nbc * ngroups + g * tiles + (j - nbc);
 }
 
-// Thread 0: wait until the chain's earlier launches are done with shot group
-// `grp`, then order the tensor loads after their stores.  False when the
-// wait ran out or another CTA raised the error word.
+// One thread of the CTA (lane 0 of warp 1 in the interior tiles, thread 0 in
+// the boundary CTAs): wait until the chain's earlier launches are done with
+// shot group `grp`, then order this thread's tensor loads after their stores
+// (the thread that issues the first copies fences again after the CTA
+// barrier).  False when the wait ran out or another CTA raised the error
+// word.
 __device__ __forceinline__ bool chain_wait(const StepArgs& a, int grp) {
     if (a.chain == nullptr || a.chain_k <= 0) return true;
     const bool ok = wait_count(a.chain + grp, (unsigned)a.chain_k * (unsigned)a.chain_per_group, a.err);
