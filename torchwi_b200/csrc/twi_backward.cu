@@ -105,26 +105,6 @@ __device__ __forceinline__ void backward_boundary(const StepArgs& a, int b, int 
     chain_done(a, grp);
 }
 
-// x neighbours of a lane's four columns at distance 1..NE from warp shuffles;
-// lanes 0 and 31 read them from the staged row `row` (haloed layout).
-template <int NE>
-__device__ __forceinline__ void x_neighbours(const float (&c4)[4], const float* row, int cs, int lane,
-                                             float (&L)[NE], float (&R)[NE]) {
-#pragma unroll
-    for (int k = 0; k < NE; ++k) {
-        L[k] = __shfl_up_sync(0xffffffffu, c4[3 - k], 1);
-        R[k] = __shfl_down_sync(0xffffffffu, c4[k], 1);
-    }
-    if (lane == 0) {
-#pragma unroll
-        for (int k = 0; k < NE; ++k) L[k] = row[cs - 1 - k];
-    }
-    if (lane == 31) {
-#pragma unroll
-        for (int k = 0; k < NE; ++k) R[k] = row[cs + 4 + k];
-    }
-}
-
 // Interior update of a lane's four cells from a (2*NE+1)-row window.
 template <int ORDER, bool EXACT>
 __device__ __forceinline__ void update4(const float4 (&win)[ORDER + 1], const float (&c4)[4],
@@ -329,7 +309,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
                 // ---- u^{it-1}: the forward update run backwards
                 const float cu[4] = {wu[NE].x, wu[NE].y, wu[NE].z, wu[NE].w};
                 float Lu[NE], Ru[NE];
-                x_neighbours<NE>(cu, uc_s + (rl + HZ) * kBoxX, cs, lane, Lu, Ru);
+                row_neighbours<NE>(uc_s + (rl + HZ) * kBoxX, cs, Lu, Ru);
                 const float4 up4 = ld4(up_s + rl * kTileX + 4 * lane);
                 const float up[4] = {up4.x, up4.y, up4.z, up4.w};
                 // u^{it+1} with the source that step `it` added taken off again
@@ -350,7 +330,7 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
                 // ---- lambda step it
                 const float cl[4] = {wl[NE].x, wl[NE].y, wl[NE].z, wl[NE].w};
                 float Ll[NE], Rl[NE];
-                x_neighbours<NE>(cl, lc_s + (rl + HZ) * kBoxX, cs, lane, Ll, Rl);
+                row_neighbours<NE>(lc_s + (rl + HZ) * kBoxX, cs, Ll, Rl);
                 const float4 lp4 = ld4(lp_s + rl * kTileX + 4 * lane);
                 const float lp[4] = {lp4.x, lp4.y, lp4.z, lp4.w};
                 float lo[4];

@@ -15,8 +15,8 @@
 //   * the gradient term -virt * lambda with Kahan or plain accumulation
 //     (adjoint).
 // Each warp streams RZ consecutive rows: a (2*NE+1)-row register window of
-// float4s along z, and warp shuffles for the x neighbours (lanes 0 and 31
-// read the x halo from shared memory).  Rows/columns of the pads use the
+// float4s along z, and the x neighbours read from the staged row (two vector
+// loads per row, the halo covering the first and last lanes).  Rows/columns of the pads use the
 // general per-cell path.  The top NE rows are the free surface: always 0.
 #include <atomic>
 #include <cstdio>
@@ -365,19 +365,7 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
             win[2 * NE] = ld4(u2s + (rl + HZ + NE) * kBoxX + cs);
             const float c4[4] = {win[NE].x, win[NE].y, win[NE].z, win[NE].w};
             float L[NE], Rr[NE];   // L[k]: column c-1-k, Rr[k]: column c+4+k
-#pragma unroll
-            for (int kk = 0; kk < NE; ++kk) {
-                L[kk] = __shfl_up_sync(0xffffffffu, c4[3 - kk], 1);
-                Rr[kk] = __shfl_down_sync(0xffffffffu, c4[kk], 1);
-            }
-            if (lane == 0) {
-#pragma unroll
-                for (int kk = 0; kk < NE; ++kk) L[kk] = u2s[(rl + HZ) * kBoxX + cs - 1 - kk];
-            }
-            if (lane == 31) {
-#pragma unroll
-                for (int kk = 0; kk < NE; ++kk) Rr[kk] = u2s[(rl + HZ) * kBoxX + cs + 4 + kk];
-            }
+            row_neighbours<NE>(u2s + (rl + HZ) * kBoxX, cs, L, Rr);
             const float4 um4 = ld4(u1s + rl * kTileX + 4 * lane);
             const float um[4] = {um4.x, um4.y, um4.z, um4.w};
             float* dst = a.fields + (long long)(d.next_base + s * d.next_stride) * a.slot_elems +

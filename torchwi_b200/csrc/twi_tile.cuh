@@ -77,6 +77,30 @@ __device__ __forceinline__ int job_of(Begin begin, int njobs, int cta) {
     return lo;
 }
 
+// x neighbours of a lane's four columns at distance 1..NE (L[k]: column
+// c-1-k, R[k]: column c+4+k), read from the staged row `row` in the haloed
+// layout (the lane's first column at `cs`, a kHaloX-column halo on each
+// side): two vector loads instead of shuffles, and no special case for the
+// first and last lanes, whose neighbours sit in the halo.
+template <int NE>
+__device__ __forceinline__ void row_neighbours(const float* row, int cs, float (&L)[NE], float (&R)[NE]) {
+    static_assert(NE == 1 || NE == 2 || NE == 4, "orders 2, 4 and 8");
+    if constexpr (NE == 1) {
+        L[0] = row[cs - 1];
+        R[0] = row[cs + 4];
+    } else if constexpr (NE == 2) {
+        const float2 l = *reinterpret_cast<const float2*>(row + cs - 2);
+        const float2 r = *reinterpret_cast<const float2*>(row + cs + 4);
+        L[0] = l.y, L[1] = l.x;
+        R[0] = r.x, R[1] = r.y;
+    } else {
+        const float4 l = ld4(row + cs - 4);
+        const float4 r = ld4(row + cs + 4);
+        L[0] = l.w, L[1] = l.z, L[2] = l.y, L[3] = l.x;
+        R[0] = r.x, R[1] = r.y, R[2] = r.z, R[3] = r.w;
+    }
+}
+
 // Shot stages consumed warp by warp.  Every warp waits for a stage's copies
 // itself (all lanes, so each sees the data; the answer is warp-uniform), and
 // the last of the CTA's `nwarps` warps to finish shot k with stage k % stages
