@@ -56,3 +56,36 @@ def test_batch_equals_plans_alone(accumulate, graphs, rz, recon, chained):
         for k in range(len(surveys)):
             assert bits_equal(gathers[k].cpu().numpy(), alone[k][0]), (rep, k)
             assert bits_equal(grads[k].cpu().numpy(), alone[k][1]), (rep, k)
+
+
+@pytest.mark.parametrize("recon", [False, True])
+def test_batch_order8_equals_plans_alone(recon):
+    """Order 8 through the multi-plan kernels, which read their step arguments
+    from shared memory (the widest register window of the three orders)."""
+    cases = [dict(nx=70, nz=33, nt=90, nshots=3, seed=4), dict(nx=101, nz=45, nt=70, nshots=5, seed=5)]
+    surveys = [synthetic.small_case(order=8, **c) for c in cases]
+
+    def plan8(s, opts):
+        p = ShotPlan(s.nx, s.nz, s.h, s.dt, s.nt, 8, nshots=s.nshots, options=opts)
+        p.set_wavelet(torch.from_numpy(s.w))
+        p.set_shots(s.sx, s.sy, s.ry)
+        p.set_model(torch.from_numpy(s.vel_start))
+        return p
+
+    opts = PlanOptions(ckpt_interval=11, reconstruct=recon, chained=False)
+    alone = []
+    for s in surveys:
+        p = plan8(s, opts)
+        frd = p.forward(save_checkpoints=True).clone()
+        alone.append((frd.cpu().numpy(), p.gradient(0.25 * frd).clone().cpu().numpy()))
+    plans = [plan8(s, PlanOptions(ckpt_interval=11, reconstruct=recon)) for s in surveys]
+    batch = PlanBatch(plans)
+    gathers = [g.clone() for g in batch.forward(save_checkpoints=True)]
+    for p, g in zip(plans, gathers):
+        p.resid.copy_(0.25 * g)
+    grads = [g.clone() for g in batch.gradient()]
+    batch.check()
+    for k in range(len(surveys)):
+        assert np.isfinite(grads[k].cpu().numpy()).all()
+        assert bits_equal(gathers[k].cpu().numpy(), alone[k][0]), k
+        assert bits_equal(grads[k].cpu().numpy(), alone[k][1]), k

@@ -292,107 +292,123 @@ __device__ __forceinline__ void backward_body(const CUtensorMap* tm_c, const CUt
 
         float* const un_slot = a.fields + slot_off(a, a.next_base, a.next_stride, s);
         float* const ln_slot = a.fields + slot_off(a, a.lnext_base, a.lnext_stride, s);
+        // PLAIN: every row of this warp is an interior row that holds neither the
+        // source nor the receivers (neither pad nor free-surface rows), so the
+        // rows run without any per-row test
+        auto rows = [&](auto plain_tag) {
+            constexpr bool PLAIN = decltype(plain_tag)::value;
 #pragma unroll
-        for (int rr = 0; rr < RZ; ++rr) {
-            const int rl = rl0 + rr;
-            const int r = z0 + rl;
-            // the bottom pad rows and everything below belong to the boundary CTAs
-            if (r >= a.dimz - NE) break;
-            wu[2 * NE] = ld4(uc_s + (rl + HZ + NE) * kBoxX + cs);
-            wl[2 * NE] = ld4(lc_s + (rl + HZ + NE) * kBoxX + cs);
-            const long long roff = (long long)r * a.pitch + c;
-            // One interior row.  FAST: neither the source nor the receiver
-            // row, so no per-row special case is tested; in the edge tiles the
-            // lanes holding pad columns mask their stores.
-            auto interior_row = [&](auto fast_tag) {
-                constexpr bool FAST = decltype(fast_tag)::value;
-                // ---- u^{it-1}: the forward update run backwards
-                const float cu[4] = {wu[NE].x, wu[NE].y, wu[NE].z, wu[NE].w};
-                float Lu[NE], Ru[NE];
-                row_neighbours<NE>(uc_s + (rl + HZ) * kBoxX, cs, Lu, Ru);
-                const float4 up4 = ld4(up_s + rl * kTileX + 4 * lane);
-                const float up[4] = {up4.x, up4.y, up4.z, up4.w};
-                // u^{it+1} with the source that step `it` added taken off again
-                float ui[4] = {up[0], up[1], up[2], up[3]};
-                if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
-                    const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-#pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        if (c + m == src_c) ui[m] = __fsub_rn(up[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int rl = rl0 + rr;
+                const int r = z0 + rl;
+                // the bottom pad rows and everything below belong to the boundary CTAs
+                if constexpr (!PLAIN) {
+                    if (r >= a.dimz - NE) break;
                 }
-                float uo[4];
-                update4<ORDER, EXACT>(wu, cu, Lu, Ru, ui, vvreg[rr], uo);
-                if (a.it < 2) {   // u^0 = u^{-1} = 0 exactly
+                wu[2 * NE] = ld4(uc_s + (rl + HZ + NE) * kBoxX + cs);
+                wl[2 * NE] = ld4(lc_s + (rl + HZ + NE) * kBoxX + cs);
+                const long long roff = (long long)r * a.pitch + c;
+                // One interior row.  FAST: neither the source nor the receiver
+                // row, so no per-row special case is tested; in the edge tiles the
+                // lanes holding pad columns mask their stores.
+                auto interior_row = [&](auto fast_tag) {
+                    constexpr bool FAST = decltype(fast_tag)::value;
+                    // ---- u^{it-1}: the forward update run backwards
+                    const float cu[4] = {wu[NE].x, wu[NE].y, wu[NE].z, wu[NE].w};
+                    float Lu[NE], Ru[NE];
+                    row_neighbours<NE>(uc_s + (rl + HZ) * kBoxX, cs, Lu, Ru);
+                    const float4 up4 = ld4(up_s + rl * kTileX + 4 * lane);
+                    const float up[4] = {up4.x, up4.y, up4.z, up4.w};
+                    // u^{it+1} with the source that step `it` added taken off again
+                    float ui[4] = {up[0], up[1], up[2], up[3]};
+                    if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
+                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) uo[m] = 0.f;
-                }
-
-                // ---- lambda step it
-                const float cl[4] = {wl[NE].x, wl[NE].y, wl[NE].z, wl[NE].w};
-                float Ll[NE], Rl[NE];
-                row_neighbours<NE>(lc_s + (rl + HZ) * kBoxX, cs, Ll, Rl);
-                const float4 lp4 = ld4(lp_s + rl * kTileX + 4 * lane);
-                const float lp[4] = {lp4.x, lp4.y, lp4.z, lp4.w};
-                float lo[4];
-                update4<ORDER, EXACT>(wl, cl, Ll, Rl, lp, vvreg[rr], lo);
-                if (!FAST && r == rec_r) {   // adjoint source on the receiver row
-                    const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-                    const float* rs = a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const int cc = c + m;
-                        if (cc >= NE && cc < NE + a.nx)
-                            lo[m] = add_injection<EXACT>(lo[m], rs[cc - NE], comp(v4, m), a.dt2);
+                        for (int m = 0; m < 4; ++m)
+                            if (c + m == src_c) ui[m] = __fsub_rn(up[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
                     }
-                }
-
-                // pad columns belong to the boundary CTAs: store interior cells only
-                if (cols_interior) {
-                    *reinterpret_cast<float4*>(un_slot + roff) = make_float4(uo[0], uo[1], uo[2], uo[3]);
-                    *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-                } else {
+                    float uo[4];
+                    update4<ORDER, EXACT>(wu, cu, Lu, Ru, ui, vvreg[rr], uo);
+                    if (a.it < 2) {   // u^0 = u^{-1} = 0 exactly
 #pragma unroll
-                    for (int m = 0; m < 4; ++m)
-                        if (cell_in[m]) un_slot[roff + m] = uo[m], ln_slot[roff + m] = lo[m];
-                }
-
-                // ---- gradient: -virt * lambda with the virtual source of step it
-                if (kahan) {
-                    // every column: the pairs of pad cells and of columns
-                    // past the grid are never read (callers crop the pads)
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
-                        float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
-                        kahan_add(sm, cm, grad_term<EXACT>(vt, lo[m]));
-                        set_comp(gsum[rr], m, sm);
-                        set_comp(gcmp[rr], m, cm);
+                        for (int m = 0; m < 4; ++m) uo[m] = 0.f;
                     }
-                } else {
-                    float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + roff;
+
+                    // ---- lambda step it
+                    const float cl[4] = {wl[NE].x, wl[NE].y, wl[NE].z, wl[NE].w};
+                    float Ll[NE], Rl[NE];
+                    row_neighbours<NE>(lc_s + (rl + HZ) * kBoxX, cs, Ll, Rl);
+                    const float4 lp4 = ld4(lp_s + rl * kTileX + 4 * lane);
+                    const float lp[4] = {lp4.x, lp4.y, lp4.z, lp4.w};
+                    float lo[4];
+                    update4<ORDER, EXACT>(wl, cl, Ll, Rl, lp, vvreg[rr], lo);
+                    if (!FAST && r == rec_r) {   // adjoint source on the receiver row
+                        const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                        const float* rs = a.resid + (long long)s * a.resid_stride + (long long)a.it * a.nx;
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        if (cell_in[m]) {
-                            const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
-                            g[m] = __fadd_rn(g[m], grad_term<EXACT>(vt, lo[m]));
+                        for (int m = 0; m < 4; ++m) {
+                            const int cc = c + m;
+                            if (cc >= NE && cc < NE + a.nx)
+                                lo[m] = add_injection<EXACT>(lo[m], rs[cc - NE], comp(v4, m), a.dt2);
                         }
                     }
-                }
-            };
-            if (r < NE) {
-                // free surface: both fields stay zero (the reference never writes these rows)
-                if (col_ok) {
-                    *reinterpret_cast<float4*>(un_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
-                    *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-            } else if (r != src_r && r != rec_r) {
-                interior_row(std::true_type{});
-            } else {
-                interior_row(std::false_type{});
-            }
+
+                    // pad columns belong to the boundary CTAs: store interior cells only
+                    if (cols_interior) {
+                        *reinterpret_cast<float4*>(un_slot + roff) = make_float4(uo[0], uo[1], uo[2], uo[3]);
+                        *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+                    } else {
 #pragma unroll
-            for (int j = 0; j < 2 * NE; ++j) wu[j] = wu[j + 1], wl[j] = wl[j + 1];
-        }
+                        for (int m = 0; m < 4; ++m)
+                            if (cell_in[m]) un_slot[roff + m] = uo[m], ln_slot[roff + m] = lo[m];
+                    }
+
+                    // ---- gradient: -virt * lambda with the virtual source of step it
+                    if (kahan) {
+                        // every column: the pairs of pad cells and of columns
+                        // past the grid are never read (callers crop the pads)
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
+                            float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                            kahan_add(sm, cm, grad_term<EXACT>(vt, lo[m]));
+                            set_comp(gsum[rr], m, sm);
+                            set_comp(gcmp[rr], m, cm);
+                        }
+                    } else {
+                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems + roff;
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) {
+                            if (cell_in[m]) {
+                                const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), uo[m], cu[m], up[m]);
+                                g[m] = __fadd_rn(g[m], grad_term<EXACT>(vt, lo[m]));
+                            }
+                        }
+                    }
+                };
+                if constexpr (PLAIN) {
+                    interior_row(std::true_type{});
+                } else if (r < NE) {
+                    // free surface: both fields stay zero (the reference never writes these rows)
+                    if (col_ok) {
+                        *reinterpret_cast<float4*>(un_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
+                        *reinterpret_cast<float4*>(ln_slot + roff) = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
+                } else if (r != src_r && r != rec_r) {
+                    interior_row(std::true_type{});
+                } else {
+                    interior_row(std::false_type{});
+                }
+#pragma unroll
+                for (int j = 0; j < 2 * NE; ++j) wu[j] = wu[j + 1], wl[j] = wl[j + 1];
+            }
+        };
+        const int rw0 = z0 + rl0;   // first row of this warp
+        if (rw0 >= NE && rw0 + RZ <= a.dimz - NE && (src_r < rw0 || src_r >= rw0 + RZ) &&
+            (rec_r < rw0 || rec_r >= rw0 + RZ))
+            rows(std::true_type{});
+        else
+            rows(std::false_type{});
 
         if (last_warp_done(sh_done, k, STAGES, WZ) && k + STAGES < nloc) issue(k + STAGES);
     }

@@ -138,7 +138,7 @@ __device__ __forceinline__ void boundary_part(const StepArgs& a, const StepDyn& 
 // boundary CTAs first, then the interior tiles.  tm_u2 / tm_u1 / tm_vel may
 // live in parameter space (single-plan kernel) or global memory (multi-plan
 // kernel).
-template <int ORDER, bool EXACT, int MODE, int RZ, int WZ>
+template <int ORDER, bool EXACT, int MODE, int RZ, int WZ, bool PLAIN_ROWS = true>
 __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUtensorMap* tm_u1p,
                                           const CUtensorMap* tm_velp, const StepArgs& a,
                                           const StepDyn& d, const int nbc, const int cta_in) {
@@ -356,240 +356,256 @@ __device__ __forceinline__ void step_body(const CUtensorMap* tm_u2p, const CUten
 #pragma unroll
         for (int j = 0; j < 2 * NE; ++j) win[j] = ld4(u2s + (rl0 + HZ - NE + j) * kBoxX + cs);
 
+        // PLAIN: every row of this warp is an interior row that holds neither the
+        // source nor the receivers (neither pad nor free-surface rows), so the
+        // rows run without any per-row test
+        auto rows = [&](auto plain_tag) {
+            constexpr bool PLAIN = decltype(plain_tag)::value;
 #pragma unroll
-        for (int rr = 0; rr < RZ; ++rr) {
-            const int rl = rl0 + rr;
-            const int r = z0 + rl;
-            // the bottom pad rows and everything below belong to the boundary CTAs
-            if (r >= a.dimz - NE) break;
-            win[2 * NE] = ld4(u2s + (rl + HZ + NE) * kBoxX + cs);
-            const float c4[4] = {win[NE].x, win[NE].y, win[NE].z, win[NE].w};
-            float L[NE], Rr[NE];   // L[k]: column c-1-k, Rr[k]: column c+4+k
-            row_neighbours<NE>(u2s + (rl + HZ) * kBoxX, cs, L, Rr);
-            const float4 um4 = ld4(u1s + rl * kTileX + 4 * lane);
-            const float um[4] = {um4.x, um4.y, um4.z, um4.w};
-            float* dst = a.fields + (long long)(d.next_base + s * d.next_stride) * a.slot_elems +
-                         (long long)r * a.pitch + c;
+            for (int rr = 0; rr < RZ; ++rr) {
+                const int rl = rl0 + rr;
+                const int r = z0 + rl;
+                // the bottom pad rows and everything below belong to the boundary CTAs
+                if (!PLAIN && r >= a.dimz - NE) break;
+                win[2 * NE] = ld4(u2s + (rl + HZ + NE) * kBoxX + cs);
+                const float c4[4] = {win[NE].x, win[NE].y, win[NE].z, win[NE].w};
+                float L[NE], Rr[NE];   // L[k]: column c-1-k, Rr[k]: column c+4+k
+                row_neighbours<NE>(u2s + (rl + HZ) * kBoxX, cs, L, Rr);
+                const float4 um4 = ld4(u1s + rl * kTileX + 4 * lane);
+                const float um[4] = {um4.x, um4.y, um4.z, um4.w};
+                float* dst = a.fields + (long long)(d.next_base + s * d.next_stride) * a.slot_elems +
+                             (long long)r * a.pitch + c;
 
-            if (r < NE) {
-                // free surface: the top rows stay zero (the reference never writes them)
-                if (col_ok) *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
-                if constexpr (MODE == kModeAdjoint) {
-                    // the excitation-amplitude assignment covers every cell of the
-                    // grid, these rows and their corner pad cells included
-                    // (td2d_cuda.cu:197-205): -exa * 0 there
-                    if (a.acc_mode == kAccExa && col_ok) {
-                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
-                        float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                                   (long long)r * a.pitch + c;
-#pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (c + m < a.dimx && a.iexa[e0 + m] == d.it)
-                                g[m] = grad_term<EXACT>(a.exa[e0 + m], 0.f);
-                    }
-                }
-                if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
-                    if (col_ok) {
-                        float vo[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            vo[m] = MODE == kModeReverse
-                                        ? virt_from_coef<EXACT>(comp(qreg[rr], m), 0.f, c4[m], um[m])
-                                        : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
-                        float* p = a.virt_out +
-                                   (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
-                                   (long long)r * a.virt_pitch + c;
-                        if (a.virt_vec4) {
-                            *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
-                        } else {
+                if (!PLAIN && r < NE) {
+                    // free surface: the top rows stay zero (the reference never writes them)
+                    if (col_ok) *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if constexpr (MODE == kModeAdjoint) {
+                        // the excitation-amplitude assignment covers every cell of the
+                        // grid, these rows and their corner pad cells included
+                        // (td2d_cuda.cu:197-205): -exa * 0 there
+                        if (a.acc_mode == kAccExa && col_ok) {
+                            const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                            float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                       (long long)r * a.pitch + c;
 #pragma unroll
                             for (int m = 0; m < 4; ++m)
-                                if (c + m < a.dimx) p[m] = vo[m];
+                                if (c + m < a.dimx && a.iexa[e0 + m] == d.it)
+                                    g[m] = grad_term<EXACT>(a.exa[e0 + m], 0.f);
                         }
                     }
-                }
-            } else {
-                // One interior row.  FAST: neither the source nor the receiver
-                // row, so no per-row special case is tested; in the edge tiles
-                // the lanes holding pad columns mask their stores.
-                auto interior_row = [&](auto fast_tag) {
-                    constexpr bool FAST = decltype(fast_tag)::value;
-                    float out[4];
-                    // backwards, u^{it+1} stands where u^{n-1} did, with the source
-                    // that step `it` added taken off again
-                    float ui[4] = {um[0], um[1], um[2], um[3]};
-                    if constexpr (MODE == kModeReverse) {
-                        if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
-                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                    if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
+                        if (col_ok) {
+                            float vo[4];
 #pragma unroll
                             for (int m = 0; m < 4; ++m)
-                                if (c + m == src_c) ui[m] = __fsub_rn(um[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
-                        }
-                    }
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        float lf[NE], rt[NE], up[NE], dn[NE];
-#pragma unroll
-                        for (int dist = 1; dist <= NE; ++dist) {
-                            const int jl = m - dist, jr = m + dist;
-                            lf[dist - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
-                            rt[dist - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
-                            up[dist - 1] = comp(win[NE - dist], m);
-                            dn[dist - 1] = comp(win[NE + dist], m);
-                        }
-                        out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
-                                                               comp(vvreg[rr], m));
-                        if constexpr (MODE == kModeReverse) {
-                            if (d.it < 2) out[m] = 0.f;   // u^0 = u^{-1} = 0 exactly
-                        }
-                    }
-                    // sources land on interior cells only (validated on the host)
-                    if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
-                        if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
-                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-#pragma unroll
-                            for (int m = 0; m < 4; ++m)
-                                if (c + m == src_c)
-                                    out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
-                        }
-                    } else if constexpr (MODE == kModeAdjoint) {
-                        if (!FAST && r == rec_r) {
-                            const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
-                            const float* rs =
-                                a.resid + (long long)s * a.resid_stride + (long long)d.it * a.nx;
-#pragma unroll
-                            for (int m = 0; m < 4; ++m) {
-                                const int cc = c + m;
-                                if (cc >= NE && cc < NE + a.nx)
-                                    out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
-                            }
-                        }
-                    }
-
-                    // pad columns belong to the boundary CTAs: store interior cells only
-                    if (cols_interior) {
-                        *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
-                    } else {
-#pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            if (cell_in[m]) dst[m] = out[m];
-                    }
-
-                    if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
-                        if (!FAST && a.frd != nullptr && r == rec_r) {
-                            const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
-                            float* g = a.frd + o;
-                            if (a.obs != nullptr) {   // the residual, one rounding like frd - obs
-                                const float* ob = a.obs + o;
-#pragma unroll
-                                for (int m = 0; m < 4; ++m) {
-                                    const int cc = c + m;
-                                    if (cc >= NE && cc < NE + a.nx) g[cc - NE] = __fsub_rn(out[m], ob[cc - NE]);
-                                }
+                                vo[m] = MODE == kModeReverse
+                                            ? virt_from_coef<EXACT>(comp(qreg[rr], m), 0.f, c4[m], um[m])
+                                            : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], 0.f);
+                            float* p = a.virt_out +
+                                       (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                       (long long)r * a.virt_pitch + c;
+                            if (a.virt_vec4) {
+                                *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
                             } else {
 #pragma unroll
-                                for (int m = 0; m < 4; ++m) {
-                                    const int cc = c + m;
-                                    if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
-                                }
+                                for (int m = 0; m < 4; ++m)
+                                    if (c + m < a.dimx) p[m] = vo[m];
                             }
                         }
                     }
-
-                    if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
-                        float vo[4];
+                } else {
+                    // One interior row.  FAST: neither the source nor the receiver
+                    // row, so no per-row special case is tested; in the edge tiles
+                    // the lanes holding pad columns mask their stores.
+                    auto interior_row = [&](auto fast_tag) {
+                        constexpr bool FAST = decltype(fast_tag)::value;
+                        float out[4];
+                        // backwards, u^{it+1} stands where u^{n-1} did, with the source
+                        // that step `it` added taken off again
+                        float ui[4] = {um[0], um[1], um[2], um[3]};
+                        if constexpr (MODE == kModeReverse) {
+                            if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
+                                const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
-                        for (int m = 0; m < 4; ++m)
-                            vo[m] = MODE == kModeReverse
-                                        ? virt_from_coef<EXACT>(comp(qreg[rr], m), out[m], c4[m], um[m])
-                                        : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
-                        float* p = a.virt_out +
-                                   (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
-                                   (long long)r * a.virt_pitch + c;
-                        if (cols_interior && a.virt_vec4) {
-                            *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
-                        } else {
-#pragma unroll
-                            for (int m = 0; m < 4; ++m)
-                                if (cell_in[m]) p[m] = vo[m];
+                                for (int m = 0; m < 4; ++m)
+                                    if (c + m == src_c) ui[m] = __fsub_rn(um[m], injection<EXACT>(wamp, comp(v4, m), a.dt2));
+                            }
                         }
-                    }
-
-                    if constexpr (MODE == kModeExaForward) {
-                        const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
-                        float4 ev = ld4(a.exa + e0);
-                        short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
-                        bool changed = false;
 #pragma unroll
                         for (int m = 0; m < 4; ++m) {
-                            if (!cell_in[m]) continue;
-                            const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
-                            if (fabsf(vt) > fabsf(comp(ev, m))) {
-                                set_comp(ev, m, vt);
-                                if (m == 0) iv.x = static_cast<short>(d.it);
-                                else if (m == 1) iv.y = static_cast<short>(d.it);
-                                else if (m == 2) iv.z = static_cast<short>(d.it);
-                                else iv.w = static_cast<short>(d.it);
-                                changed = true;
+                            float lf[NE], rt[NE], up[NE], dn[NE];
+#pragma unroll
+                            for (int dist = 1; dist <= NE; ++dist) {
+                                const int jl = m - dist, jr = m + dist;
+                                lf[dist - 1] = jl >= 0 ? c4[jl] : L[-jl - 1];
+                                rt[dist - 1] = jr < 4 ? c4[jr] : Rr[jr - 4];
+                                up[dist - 1] = comp(win[NE - dist], m);
+                                dn[dist - 1] = comp(win[NE + dist], m);
+                            }
+                            out[m] = interior_update<ORDER, EXACT>(lf, rt, up, dn, c4[m], ui[m],
+                                                                   comp(vvreg[rr], m));
+                            if constexpr (MODE == kModeReverse) {
+                                if (d.it < 2) out[m] = 0.f;   // u^0 = u^{-1} = 0 exactly
                             }
                         }
-                        if (changed) {
-                            if (cols_interior) {
-                                *reinterpret_cast<float4*>(a.exa + e0) = ev;
-                                *reinterpret_cast<short4*>(a.iexa + e0) = iv;
-                            } else {   // pad columns belong to the boundary CTAs
-                                const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+                        // sources land on interior cells only (validated on the host)
+                        if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
+                            if (!FAST && r == src_r && src_c >= c && src_c < c + 4) {
+                                const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
 #pragma unroll
                                 for (int m = 0; m < 4; ++m)
-                                    if (cell_in[m]) a.exa[e0 + m] = comp(ev, m), a.iexa[e0 + m] = is[m];
+                                    if (c + m == src_c)
+                                        out[m] = add_injection<EXACT>(out[m], wamp, comp(v4, m), a.dt2);
+                            }
+                        } else if constexpr (MODE == kModeAdjoint) {
+                            if (!FAST && r == rec_r) {
+                                const float4 v4 = ld4(vs + rl * kTileX + 4 * lane);
+                                const float* rs =
+                                    a.resid + (long long)s * a.resid_stride + (long long)d.it * a.nx;
+#pragma unroll
+                                for (int m = 0; m < 4; ++m) {
+                                    const int cc = c + m;
+                                    if (cc >= NE && cc < NE + a.nx)
+                                        out[m] = add_injection<EXACT>(out[m], rs[cc - NE], comp(v4, m), a.dt2);
+                                }
                             }
                         }
-                    }
 
-                    if constexpr (MODE == kModeAdjoint) {
-                        if (a.acc_mode == kAccExa) {
-                            const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
-                            const short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
-                            const short is[4] = {iv.x, iv.y, iv.z, iv.w};
-                            float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                                       (long long)r * a.pitch + c;
+                        // pad columns belong to the boundary CTAs: store interior cells only
+                        if (cols_interior) {
+                            *reinterpret_cast<float4*>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+                        } else {
 #pragma unroll
                             for (int m = 0; m < 4; ++m)
-                                if (cell_in[m] && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
-                        } else if (a.acc_mode == kAccKahanPerGroup) {
-                            // every column: the pairs of pad cells and of columns
-                            // past the grid are never read (callers crop the pads)
+                                if (cell_in[m]) dst[m] = out[m];
+                        }
+
+                        if constexpr (MODE != kModeAdjoint && MODE != kModeReverse) {
+                            if (!FAST && a.frd != nullptr && r == rec_r) {
+                                const long long o = (long long)s * a.frd_stride + (long long)d.it * a.nx;
+                                float* g = a.frd + o;
+                                if (a.obs != nullptr) {   // the residual, one rounding like frd - obs
+                                    const float* ob = a.obs + o;
 #pragma unroll
-                            for (int m = 0; m < 4; ++m) {
-                                float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
-                                kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
-                                set_comp(gsum[rr], m, sm);
-                                set_comp(gcmp[rr], m, cm);
+                                    for (int m = 0; m < 4; ++m) {
+                                        const int cc = c + m;
+                                        if (cc >= NE && cc < NE + a.nx) g[cc - NE] = __fsub_rn(out[m], ob[cc - NE]);
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int m = 0; m < 4; ++m) {
+                                        const int cc = c + m;
+                                        if (cc >= NE && cc < NE + a.nx) g[cc - NE] = out[m];
+                                    }
+                                }
                             }
-                        } else if (a.acc_mode == kAccPlainPerShot) {
-                            float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
-                                       (long long)r * a.pitch + c;
-                            if (cols_interior) {
-                                float4 gv = ld4(g);
+                        }
+
+                        if constexpr (MODE == kModeRecompute || MODE == kModeReverse) {
+                            float vo[4];
 #pragma unroll
-                                for (int m = 0; m < 4; ++m)
-                                    set_comp(gv, m, __fadd_rn(comp(gv, m),
-                                                              grad_term<EXACT>(comp(vin[rr], m), out[m])));
-                                *reinterpret_cast<float4*>(g) = gv;
+                            for (int m = 0; m < 4; ++m)
+                                vo[m] = MODE == kModeReverse
+                                            ? virt_from_coef<EXACT>(comp(qreg[rr], m), out[m], c4[m], um[m])
+                                            : virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                            float* p = a.virt_out +
+                                       (long long)(d.virt_base + s * a.virt_stride) * a.virt_slot_elems +
+                                       (long long)r * a.virt_pitch + c;
+                            if (cols_interior && a.virt_vec4) {
+                                *reinterpret_cast<float4*>(p) = make_float4(vo[0], vo[1], vo[2], vo[3]);
                             } else {
 #pragma unroll
                                 for (int m = 0; m < 4; ++m)
-                                    if (cell_in[m])
-                                        g[m] = __fadd_rn(g[m], grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                    if (cell_in[m]) p[m] = vo[m];
                             }
                         }
-                    }
-                };
-                if (r != src_r && r != rec_r) interior_row(std::true_type{});
-                else interior_row(std::false_type{});
-            }
+
+                        if constexpr (MODE == kModeExaForward) {
+                            const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                            float4 ev = ld4(a.exa + e0);
+                            short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                            bool changed = false;
 #pragma unroll
-            for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
+                            for (int m = 0; m < 4; ++m) {
+                                if (!cell_in[m]) continue;
+                                const float vt = virt_from_coef<EXACT>(comp(qreg[rr], m), um[m], c4[m], out[m]);
+                                if (fabsf(vt) > fabsf(comp(ev, m))) {
+                                    set_comp(ev, m, vt);
+                                    if (m == 0) iv.x = static_cast<short>(d.it);
+                                    else if (m == 1) iv.y = static_cast<short>(d.it);
+                                    else if (m == 2) iv.z = static_cast<short>(d.it);
+                                    else iv.w = static_cast<short>(d.it);
+                                    changed = true;
+                                }
+                            }
+                            if (changed) {
+                                if (cols_interior) {
+                                    *reinterpret_cast<float4*>(a.exa + e0) = ev;
+                                    *reinterpret_cast<short4*>(a.iexa + e0) = iv;
+                                } else {   // pad columns belong to the boundary CTAs
+                                    const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+#pragma unroll
+                                    for (int m = 0; m < 4; ++m)
+                                        if (cell_in[m]) a.exa[e0 + m] = comp(ev, m), a.iexa[e0 + m] = is[m];
+                                }
+                            }
+                        }
+
+                        if constexpr (MODE == kModeAdjoint) {
+                            if (a.acc_mode == kAccExa) {
+                                const long long e0 = (long long)s * a.slot_elems + (long long)r * a.pitch + c;
+                                const short4 iv = *reinterpret_cast<const short4*>(a.iexa + e0);
+                                const short is[4] = {iv.x, iv.y, iv.z, iv.w};
+                                float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                           (long long)r * a.pitch + c;
+#pragma unroll
+                                for (int m = 0; m < 4; ++m)
+                                    if (cell_in[m] && is[m] == d.it) g[m] = grad_term<EXACT>(a.exa[e0 + m], out[m]);
+                            } else if (a.acc_mode == kAccKahanPerGroup) {
+                                // every column: the pairs of pad cells and of columns
+                                // past the grid are never read (callers crop the pads)
+#pragma unroll
+                                for (int m = 0; m < 4; ++m) {
+                                    float sm = comp(gsum[rr], m), cm = comp(gcmp[rr], m);
+                                    kahan_add(sm, cm, grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                    set_comp(gsum[rr], m, sm);
+                                    set_comp(gcmp[rr], m, cm);
+                                }
+                            } else if (a.acc_mode == kAccPlainPerShot) {
+                                float* g = a.acc + (long long)(a.acc_base + s) * a.slot_elems +
+                                           (long long)r * a.pitch + c;
+                                if (cols_interior) {
+                                    float4 gv = ld4(g);
+#pragma unroll
+                                    for (int m = 0; m < 4; ++m)
+                                        set_comp(gv, m, __fadd_rn(comp(gv, m),
+                                                                  grad_term<EXACT>(comp(vin[rr], m), out[m])));
+                                    *reinterpret_cast<float4*>(g) = gv;
+                                } else {
+#pragma unroll
+                                    for (int m = 0; m < 4; ++m)
+                                        if (cell_in[m])
+                                            g[m] = __fadd_rn(g[m], grad_term<EXACT>(comp(vin[rr], m), out[m]));
+                                }
+                            }
+                        }
+                    };
+                    if (PLAIN || (r != src_r && r != rec_r)) interior_row(std::true_type{});
+                    else interior_row(std::false_type{});
+                }
+#pragma unroll
+                for (int j = 0; j < 2 * NE; ++j) win[j] = win[j + 1];
+            }
+        };
+        const int rw0 = z0 + rl0;   // first row of this warp
+        if constexpr (PLAIN_ROWS) {
+            if (rw0 >= NE && rw0 + RZ <= a.dimz - NE && (src_r < rw0 || src_r >= rw0 + RZ) &&
+                (rec_r < rw0 || rec_r >= rw0 + RZ))
+                rows(std::true_type{});
+            else
+                rows(std::false_type{});
+        } else {
+            rows(std::false_type{});
         }
 
         if (last_warp_done(sh_done, k, STAGES, WZ) && k + STAGES < nloc) issue(k + STAGES);
@@ -659,7 +675,7 @@ step_kernel_persistent(const __grid_constant__ CUtensorMap tm_u2, const __grid_c
     uint64_t* bars = reinterpret_cast<uint64_t*>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
     persistent_loop(P, bars, 1 + Smem<ORDER, RZ, WZ>::STAGES, [&](const StepArgs& a, int cta) {
-        step_body<ORDER, EXACT, MODE, RZ, WZ>(&tm_u2, &tm_u1, &tm_vel, a, dyn_of(a), P.nbc, cta);
+        step_body<ORDER, EXACT, MODE, RZ, WZ, false>(&tm_u2, &tm_u1, &tm_vel, a, dyn_of(a), P.nbc, cta);
     });
 }
 
